@@ -1,0 +1,390 @@
+#!/usr/bin/env python3
+"""Benchmark of the Wilson even-odd solve path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Workloads (seeded synthetic inputs with the shapes of the reference's
+benchmark configurations; no external data):
+  cg      (default) 32^4, links exp(i 0.3 H), kappa = 0.124, Gaussian source;
+          one step = one solve of M x = b to true residual |b - M x|/|b| <= 1e-10.
+          metric: CG solves/s.
+  dslash  32^4, the even-odd operator applied with its dagger; one step =
+          100 x (apply + dagger).  metric: dslash HBM GB/s (algorithmic bytes).
+  cg8     8^4, kappa = 0.12, plain FP64 CG (the CPU-runnable configuration).
+
+Multi-GPU runs (torchrun) are replicas: every rank solves its own copy of the
+workload; value = total solves over all ranks / max-over-ranks device time.
+`--impl reference` times the CPU oracle in the reference's loop structure
+(reference-structured even-odd operator + CG of conjugate_gradient.h) on the
+host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CG solves/s at 1e-10 residual (mixed vs FP64), dslash HBM GB/s, p50/p99 ms"
+
+WORKLOADS = {
+    "cg": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101),
+    "cg8": dict(dims=(8, 8, 8, 8), eps=0.3, kappa=0.12, tol=1e-10, link_seed=1, src_seed=2),
+    "dslash": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=None, link_seed=100, src_seed=101),
+}
+# CG iterations of one solve of each workload (FP64 CG on M^dag M, true residual 1e-10), used to turn the
+# reference arm's per-iteration time into solves/s.  Measured by the FP64 GPU CG on exactly these seeded
+# inputs; the CPU runs the same algorithm, so the count is the same.
+ITERS_PER_SOLVE = {"cg": None, "cg8": None}
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------ distributed plumbing
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend):
+        if self.world > 1:
+            import torch.distributed as dist
+            import datetime
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        import torch.distributed as dist
+        dev = f"cuda:{self.local_rank}" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        import torch.distributed as dist
+        dev = f"cuda:{self.local_rank}" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+
+def cpu_sample(workload: str, seconds_budget: float = 20.0):
+    """Reference-structured oracle on the host cores: time per CG iteration and per apply."""
+    from oracle import oracle as o
+    o.build()
+    w = WORKLOADS[workload]
+    dims = w["dims"]
+    U = o.gen_links(dims, w["eps"], w["link_seed"])
+    b = o.gen_spinor(dims, w["src_seed"], o.EVEN)
+    R = o.RefStructured(dims)
+    out = np.zeros_like(b)
+    cores = o.num_threads()
+    # one apply to estimate, then as many CG iterations as fit the budget (at least 2)
+    t0 = time.perf_counter()
+    R.eo_apply(U, w["kappa"], b, out, 1)
+    t_apply = time.perf_counter() - t0
+    n_it = max(2, min(50, int(seconds_budget / max(3 * t_apply, 1e-6))))
+    x = np.zeros_like(b)
+    t0 = time.perf_counter()
+    it, _ = R.cg(U, w["kappa"], b, x, 1e-300, n_it)
+    t_cg = time.perf_counter() - t0
+    R.close()
+    return dict(t_iter=t_cg / max(it, 1), iters=it, t_apply=t_apply, cores=cores, dims=dims)
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, dist: Dist):
+    import torch
+    import hila_b200 as hw
+    torch.cuda.set_device(dist.local_rank)
+    dist.init("nccl")
+    w = WORKLOADS[args.workload]
+    dims = w["dims"]
+    ctx = hw.Context(dist.local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    lat = hw.Lattice(ctx, dims, True)
+    U = hw.generate_links(dims, w["eps"], w["link_seed"])
+    G = hw.GaugeField(lat, U, args.link_format)
+    b_host = hw.generate_spinor(dims, w["src_seed"], hw.EVEN)
+    fb, fx = hw.Field(lat, b_host), hw.Field(lat)
+    D = hw.Dirac_Wilson_evenodd(w["kappa"], G)
+    V = int(np.prod(dims))
+    Vh = V // 2
+    peak, peak_kind = hbm_peak()
+    link_bytes = 144 if args.link_format == 18 else 96
+    # algorithmic bytes per hop launch (one output site): 8 links + neighbour spinors once + output
+    hop_bytes = 8 * link_bytes + 192 + 192
+    apply_bytes = (2 * hop_bytes + 192) * Vh  # second hop also reads in_e
+
+    def dslash_time(nrep):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fy = hw.Field(lat)
+        D.apply(fb, fy)
+        D.dagger(fy, fx)
+        ctx.synchronize()
+        ev0.record(stream)
+        for _ in range(nrep):
+            D.apply(fb, fy)
+            D.dagger(fy, fx)
+        ev1.record(stream)
+        ev1.synchronize()
+        fy.close()
+        return ev0.elapsed_time(ev1) / (2 * nrep)  # ms per eo apply
+
+    result = {}
+    clocks = ClockSampler(dist.local_rank)
+    if args.workload == "dslash":
+        nrep = 100
+        for _ in range(args.warmup):
+            dslash_time(10)
+        dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        ms = [dslash_time(nrep) for _ in range(args.steps)]
+        clk = clocks.stop()
+        ms_apply = dist.max(statistics.mean(ms))
+        gbs = apply_bytes / (ms_apply * 1e-3) / 1e9
+        value = dist.sum(gbs)
+        ms_per_step = ms_apply * 2 * nrep
+        unit = "GB/s"
+        launches = args.steps * nrep * 4
+        result["flops_per_s"] = dist.sum(1320 * V / (ms_apply * 1e-3))
+        result["ms_per_apply"] = ms_apply
+        e2e = None
+        dtype = "f64"
+        roof_ms = ms_apply
+    else:
+        def solve_once():
+            fx.zero()
+            return D.solve(fb, fx, accuracy=w["tol"], precision=args.precision)
+
+        for _ in range(args.warmup):
+            r = solve_once()
+        dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        res = [solve_once() for _ in range(args.steps)]
+        ev1.record(stream)
+        ev1.synchronize()
+        clk = clocks.stop()
+        t = dist.max(ev0.elapsed_time(ev1) * 1e-3)
+        dist.barrier()
+        value = dist.world * args.steps / t
+        ms_per_step = t / args.steps * 1e3
+        unit = "solves/s"
+        launches = sum(r.kernel_launches for r in res)
+        ok = all(r.converged for r in res)
+        result.update(iterations=res[0].iterations, true_residual=max(r.true_residual for r in res),
+                      all_converged=ok, restarts=res[0].restarts, precision=args.precision)
+        dtype = {"f64": "f64", "f32": "f32+f64", "f16": "f16+f64"}[args.precision]
+        # e2e: host arrays through the C ABI (H2D of b and D2H of x inside the timed region)
+        pb = hw.PinnedArray((V, 4, 3, 2))
+        px = hw.PinnedArray((V, 4, 3, 2))
+        pb.array[:] = b_host
+        D.solve_host(pb.array, px.array, accuracy=w["tol"], precision=args.precision)
+        dist.barrier()
+        t0 = time.perf_counter()
+        re2e = [D.solve_host(pb.array, px.array, accuracy=w["tol"], precision=args.precision)
+                for _ in range(args.steps)]
+        t_e2e = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.world * args.steps / t_e2e, "unit": "solves/s",
+               "h2d_bytes_per_step": int(pb.array.nbytes), "d2h_bytes_per_step": int(px.array.nbytes),
+               "all_converged": all(r.converged for r in re2e)}
+        pb.free()
+        px.free()
+        # dominant kernel: the hopping term; time it live on the library stream
+        roof_ms = dslash_time(50)
+        result["dslash_ms_per_apply"] = roof_ms
+    hop_ms = roof_ms / 2
+    achieved = (apply_bytes / 2) / (hop_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": None, "kernel": "k_hop (FP64, %d-real links)" % args.link_format,
+                "algorithmic_bytes_per_launch": apply_bytes / 2}
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": unit, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": dtype, "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources",
+        "config": {"workload": args.workload, "lattice": "x".join(map(str, dims)), "kappa": w["kappa"],
+                   "eps": w["eps"], "tol": w["tol"], "link_format": args.link_format,
+                   "parallelism": f"replicas{dist.world}",
+                   "l2": "inputs larger than L2 (links %d MB)" % (4 * V * link_bytes // 2**20)},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "impl": "ours",
+        **result,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and args.workload != "dslash":
+        cs = cpu_sample(args.workload)
+        iters = result.get("iterations") or 1
+        out["cpu_baseline"] = {"value": 1.0 / (cs["t_iter"] * iters), "unit": "solves/s", "cores": cs["cores"],
+                               "kind": "port",
+                               "sample": f"{cs['iters']} CG iterations of the reference-structured oracle at "
+                                         f"{'x'.join(map(str, cs['dims']))} on {cs['cores']} threads "
+                                         f"({cs['t_iter']:.3f} s/iteration), scaled by the {iters} iterations "
+                                         f"of one solve"}
+    elif dist.rank == 0 and dist.world == 1 and args.workload == "dslash" and not args.no_cpu_baseline:
+        cs = cpu_sample("cg", seconds_budget=5.0)
+        out["cpu_baseline"] = {"value": apply_bytes / cs["t_apply"] / 1e9, "unit": "GB/s", "cores": cs["cores"],
+                               "kind": "port", "sample": "one reference-structured even-odd apply at 32^4"}
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+    for f in (fb, fx):
+        f.close()
+    G.close()
+    lat.close()
+    ctx.close()
+    dist.close()
+
+
+# ------------------------------------------------------------------ reference arm
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    if args.workload == "dslash":
+        samples = [cpu_sample("cg", seconds_budget=2.0) for _ in range(args.warmup + args.steps)][args.warmup:]
+        t = statistics.mean(s["t_apply"] for s in samples)
+        V = int(np.prod(w["dims"]))
+        value = (2 * (8 * 144 + 384) + 192) * (V // 2) / t / 1e9
+        unit, cs, sample = "GB/s", samples[0], "one reference-structured even-odd apply per step"
+        ms_per_step = t * 1e3
+    else:
+        iters = ITERS_PER_SOLVE.get(args.workload)
+        samples = [cpu_sample(args.workload, seconds_budget=15.0) for _ in range(args.warmup + args.steps)]
+        samples = samples[args.warmup:]
+        t_iter = statistics.mean(s["t_iter"] for s in samples)
+        if iters is None:
+            iters = 1
+        value = 1.0 / (t_iter * iters)
+        unit, cs = "solves/s", samples[0]
+        sample = (f"{cs['iters']} CG iterations per step of the reference-structured oracle, scaled by the "
+                  f"{iters} iterations one solve of this workload takes")
+        ms_per_step = t_iter * iters * 1e3
+    out = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": dist.world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": {"workload": args.workload, "lattice": "x".join(map(str, w["dims"])), "kappa": w["kappa"]},
+           "cpu_baseline": {"value": value, "unit": unit, "cores": cs["cores"], "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="cg", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
+    ap.add_argument("--link-format", type=int, default=18, choices=[18, 12])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    dist = Dist()
+    if args.impl == "reference":
+        run_reference(args, dist)
+    else:
+        run_ours(args, dist)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,441 @@
+"""hila_b200 — B200-native Wilson-fermion solve path with HILA's interface.
+
+Python mirror of the reference's operator/solver API over the C ABI in
+``include/hila_b200.h`` (``libhila_b200.so``, built by ``hila_b200.build``):
+
+    =====================================  ===========================================
+    reference (C++)                        here
+    =====================================  ===========================================
+    lattice.setup(size)                    Lattice(ctx, dims, antiperiodic=True)
+    Field<SU<3,double>> U[NDIM]            GaugeField(lattice, links)
+    Field<Wilson_vector<3,double>>         Field(lattice)
+    Dirac_Wilson_evenodd<SU<3>> D(k, U)    Dirac_Wilson_evenodd(kappa, gauge)
+    D.apply(in, out) / D.dagger(in, out)   same
+    Dirac_Wilson<SU<3>> D(k, U)            Dirac_Wilson(kappa, gauge)
+    CG<Op> inv(D[, acc[, maxiters]])       CG(D, accuracy=1e-12, maxiters=10000)
+    inv.apply(in, out)                     same; returns a CGResult
+    =====================================  ===========================================
+
+(libraries/dirac/wilson.h:146-312, libraries/dirac/conjugate_gradient.h:18-104.)
+
+There is no CPU fallback: every operator call runs the CUDA kernels, and the
+module raises ImportError when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhila_b200.so")
+
+HW_OK = 0
+HW_ERR_INVALID = -1
+HW_ERR_OOM = -2
+HW_ERR_CUDA = -3
+HW_ERR_NOT_CONVERGED = -4
+HW_ERR_BREAKDOWN = -5
+HW_ERR_TIMEOUT = -6
+HW_ERR_REJECTED = -7
+HW_ERR_CANCELLED = -8
+HW_ERR_NO_DEVICE = -9
+
+EVEN, ODD, ALL = 1, 2, 3
+PREC_F64, PREC_F32, PREC_F16 = 0, 1, 2
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16}
+
+_STATUS_NAMES = {
+    HW_OK: "ok", HW_ERR_INVALID: "invalid argument", HW_ERR_OOM: "out of device memory",
+    HW_ERR_CUDA: "CUDA error", HW_ERR_NOT_CONVERGED: "not converged", HW_ERR_BREAKDOWN: "CG breakdown",
+    HW_ERR_TIMEOUT: "device wait timed out", HW_ERR_REJECTED: "rejected", HW_ERR_CANCELLED: "cancelled",
+    HW_ERR_NO_DEVICE: "no CUDA device",
+}
+
+
+class HilaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _CgParams(ctypes.Structure):
+    _fields_ = [("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int), ("precision", ctypes.c_int),
+                ("delta", ctypes.c_double), ("true_residual", ctypes.c_int), ("use_graph", ctypes.c_int)]
+
+
+class _CgResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int),
+                ("restarts", ctypes.c_int), ("rr_relative", ctypes.c_double), ("true_residual", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_int)]
+
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_SIGNATURES = {
+    "hw_api_version": (ctypes.c_int, []),
+    "hw_last_error": (ctypes.c_char_p, []),
+    "hw_device_count": (ctypes.c_int, [_ip]),
+    "hw_context_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "hw_context_destroy": (ctypes.c_int, [_vp]),
+    "hw_context_synchronize": (ctypes.c_int, [_vp]),
+    "hw_context_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "hw_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "hw_host_free": (ctypes.c_int, [_vp]),
+    "hw_lattice_create": (ctypes.c_int, [_vp, _ip, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "hw_lattice_destroy": (ctypes.c_int, [_vp]),
+    "hw_lattice_volume": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "hw_gauge_create": (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "hw_gauge_destroy": (ctypes.c_int, [_vp]),
+    "hw_field_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "hw_field_destroy": (ctypes.c_int, [_vp]),
+    "hw_field_upload": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_field_download": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_field_zero": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "hw_wilson_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "hw_wilson_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "hw_wilson_apply": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    "hw_wilson_hop": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "hw_cg_params_default": (None, [ctypes.POINTER(_CgParams)]),
+    "hw_cg_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.POINTER(_CgParams),
+                                   ctypes.POINTER(_CgResult)]),
+    "hw_wilson_evenodd_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.POINTER(_CgParams),
+                                               ctypes.POINTER(_CgResult)]),
+    "hw_wilson_evenodd_solve_host": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp, ctypes.POINTER(_CgParams),
+                                                    ctypes.POINTER(_CgResult)]),
+    "hw_generate_links": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_uint64, _dp]),
+    "hw_generate_spinor": (ctypes.c_int, [_ip, ctypes.c_uint64, ctypes.c_int, _dp]),
+}
+
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libhila_b200.so; raises ImportError if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hila_b200.build` "
+                              "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def lib() -> ctypes.CDLL:
+    return load_library()
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def _check(rc: int) -> int:
+    if rc != HW_OK:
+        raise HilaError(rc, lib().hw_last_error().decode(errors="replace"))
+    return rc
+
+
+def _dims(dims):
+    return (ctypes.c_int * 4)(*[int(d) for d in dims])
+
+
+def _dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)
+
+
+def device_count() -> int:
+    n = ctypes.c_int(0)
+    rc = lib().hw_device_count(ctypes.byref(n))
+    return n.value if rc == HW_OK else 0
+
+
+# ------------------------------------------------------------------ inputs
+
+def generate_links(dims, eps: float, seed: int) -> np.ndarray:
+    """Seeded SU(3) links U = exp(i eps H), shape (4, V, 3, 3, 2) float64."""
+    V = int(np.prod(dims))
+    U = np.empty((4, V, 3, 3, 2), np.float64)
+    _check(lib().hw_generate_links(_dims(dims), float(eps), int(seed), _dptr(U)))
+    return U
+
+
+def generate_spinor(dims, seed: int, parity: int = ALL) -> np.ndarray:
+    """Seeded Gaussian Wilson spinor field, shape (V, 4, 3, 2) float64."""
+    V = int(np.prod(dims))
+    psi = np.empty((V, 4, 3, 2), np.float64)
+    _check(lib().hw_generate_spinor(_dims(dims), int(seed), int(parity), _dptr(psi)))
+    return psi
+
+
+class PinnedArray:
+    """A float64 numpy array in page-locked host memory (hw_host_alloc)."""
+
+    def __init__(self, shape):
+        n = int(np.prod(shape))
+        self._ptr = _vp()
+        _check(lib().hw_host_alloc(n * 8, ctypes.byref(self._ptr)))
+        buf = (ctypes.c_double * n).from_address(self._ptr.value)
+        self.array = np.frombuffer(buf, np.float64).reshape(shape)
+
+    def free(self):
+        if self._ptr:
+            lib().hw_host_free(self._ptr)
+            self._ptr = _vp()
+            self.array = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ handles
+
+class Context:
+    """One GPU (stream, reduction buffers, graph caches)."""
+
+    def __init__(self, device: int = 0):
+        self.handle = _vp()
+        _check(lib().hw_context_create(int(device), ctypes.byref(self.handle)))
+        self.device = device
+
+    def synchronize(self):
+        _check(lib().hw_context_synchronize(self.handle))
+
+    def stream(self) -> int:
+        """The library's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        s = _vp()
+        _check(lib().hw_context_stream(self.handle, ctypes.byref(s)))
+        return s.value or 0
+
+    def close(self):
+        if self.handle:
+            lib().hw_context_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """lattice.setup(dims) (plumbing/lattice.cpp:37-104); t antiperiodic for fermions."""
+
+    def __init__(self, ctx: Context, dims, antiperiodic: bool = True):
+        self.ctx = ctx
+        self.dims = tuple(int(d) for d in dims)
+        self.volume = int(np.prod(self.dims))
+        self.handle = _vp()
+        _check(lib().hw_lattice_create(ctx.handle, _dims(self.dims), int(bool(antiperiodic)),
+                                       ctypes.byref(self.handle)))
+
+    def close(self):
+        if self.handle:
+            lib().hw_lattice_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GaugeField:
+    """Field<SU<3,double>> U[NDIM] uploaded once to the device."""
+
+    def __init__(self, lattice: Lattice, links: np.ndarray, link_format: int = 18):
+        links = np.ascontiguousarray(links, np.float64)
+        if links.size != 4 * lattice.volume * 18:
+            raise ValueError("links must hold 4*V*18 doubles")
+        self.lattice = lattice
+        self.link_format = link_format
+        self.handle = _vp()
+        _check(lib().hw_gauge_create(lattice.handle, _dptr(links), int(link_format), ctypes.byref(self.handle)))
+
+    def close(self):
+        if self.handle:
+            lib().hw_gauge_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field:
+    """Field<Wilson_vector<3,double>>: a device-resident FP64 spinor field."""
+
+    def __init__(self, lattice: Lattice, data: np.ndarray | None = None, parity: int = ALL):
+        self.lattice = lattice
+        self.handle = _vp()
+        _check(lib().hw_field_create(lattice.handle, ctypes.byref(self.handle)))
+        if data is not None:
+            self.upload(data, parity)
+
+    def upload(self, data: np.ndarray, parity: int = ALL):
+        data = np.ascontiguousarray(data, np.float64)
+        if data.size != self.lattice.volume * 24:
+            raise ValueError("spinor arrays hold V*24 doubles")
+        _check(lib().hw_field_upload(self.handle, _dptr(data), int(parity)))
+
+    def download(self, parity: int = ALL, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.lattice.volume, 4, 3, 2), np.float64)
+        _check(lib().hw_field_download(self.handle, _dptr(out), int(parity)))
+        return out
+
+    def zero(self, parity: int = ALL):
+        _check(lib().hw_field_zero(self.handle, int(parity)))
+
+    def close(self):
+        if self.handle:
+            lib().hw_field_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ operators
+
+class Dirac_Wilson_evenodd:
+    """Dirac_Wilson_evenodd<SU<3,double>> (wilson.h:234-312): M = 1 - kappa^2 H^{eo} H^{oe} on EVEN."""
+
+    par = EVEN
+
+    def __init__(self, kappa: float, gauge: GaugeField):
+        self.kappa = float(kappa)
+        self.gauge = gauge
+
+    def apply(self, inp: Field, out: Field):
+        _check(lib().hw_wilson_evenodd_apply(self.gauge.handle, self.kappa, inp.handle, out.handle))
+
+    def dagger(self, inp: Field, out: Field):
+        _check(lib().hw_wilson_evenodd_dagger(self.gauge.handle, self.kappa, inp.handle, out.handle))
+
+    def hop(self, inp: Field, out: Field, parity: int, sign: int, set_: bool = True):
+        """Dirac_Wilson_hop_set (set_) / Dirac_Wilson_hop with this operator's kappa."""
+        _check(lib().hw_wilson_hop(self.gauge.handle, self.kappa, inp.handle, out.handle, int(parity), int(sign),
+                                   int(bool(set_))))
+
+    def solve(self, b: Field, x: Field, accuracy: float = 1e-10, maxiters: int = 10000, precision: str = "f64",
+              delta: float = 0.1, use_graph: bool = True) -> "CGResult":
+        """M x = b by CG on M^dag M with source M^dag b until |b - M x|/|b| <= accuracy."""
+        p = _params(accuracy, maxiters, precision, delta, True, use_graph)
+        r = _CgResult()
+        rc = lib().hw_wilson_evenodd_solve(self.gauge.handle, self.kappa, b.handle, x.handle, ctypes.byref(p),
+                                           ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        return CGResult.from_c(r)
+
+    def solve_host(self, b: np.ndarray, x: np.ndarray, accuracy: float = 1e-10, maxiters: int = 10000,
+                   precision: str = "f64", delta: float = 0.1) -> "CGResult":
+        """Host arrays in and out (copies included in the call)."""
+        p = _params(accuracy, maxiters, precision, delta, True, True)
+        r = _CgResult()
+        rc = lib().hw_wilson_evenodd_solve_host(self.gauge.handle, self.kappa, _dptr(b), _dptr(x), ctypes.byref(p),
+                                                ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        return CGResult.from_c(r)
+
+
+class Dirac_Wilson:
+    """Dirac_Wilson<SU<3,double>> (wilson.h:146-201): D = 1 - kappa H over ALL sites."""
+
+    par = ALL
+
+    def __init__(self, kappa: float, gauge: GaugeField):
+        self.kappa = float(kappa)
+        self.gauge = gauge
+
+    def apply(self, inp: Field, out: Field):
+        _check(lib().hw_wilson_apply(self.gauge.handle, self.kappa, 1, inp.handle, out.handle))
+
+    def dagger(self, inp: Field, out: Field):
+        _check(lib().hw_wilson_apply(self.gauge.handle, self.kappa, -1, inp.handle, out.handle))
+
+
+@dataclass
+class CGResult:
+    status: int
+    iterations: int
+    reliable_updates: int
+    restarts: int
+    rr_relative: float
+    true_residual: float
+    seconds: float
+    kernel_launches: int = 0
+
+    @property
+    def converged(self) -> bool:
+        return self.status == HW_OK
+
+    @classmethod
+    def from_c(cls, r: _CgResult) -> "CGResult":
+        return cls(r.status, r.iterations, r.reliable_updates, r.restarts, r.rr_relative, r.true_residual,
+                   r.seconds, r.kernel_launches)
+
+
+def _params(accuracy, maxiters, precision, delta, true_residual, use_graph) -> _CgParams:
+    p = _CgParams()
+    lib().hw_cg_params_default(ctypes.byref(p))
+    p.accuracy = float(accuracy)
+    p.maxiters = int(maxiters)
+    p.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    p.delta = float(delta)
+    p.true_residual = int(bool(true_residual))
+    p.use_graph = int(bool(use_graph))
+    return p
+
+
+class CG:
+    """CG<Op> (conjugate_gradient.h:18-104): apply(in, out) solves (M^dag M) out = in.
+
+    Defaults follow the reference: accuracy 1e-12, maxiters 10000, stopping
+    when |r|^2 < accuracy^2 |in|^2.  ``true_residual=True`` instead continues
+    until the recomputed FP64 residual |in - M^dag M out| / |in| <= accuracy.
+    """
+
+    def __init__(self, op: Dirac_Wilson_evenodd, accuracy: float = 1e-12, maxiters: int = 10000,
+                 precision: str = "f64", true_residual: bool = False, delta: float = 0.1, use_graph: bool = True):
+        if not isinstance(op, Dirac_Wilson_evenodd):
+            raise TypeError("CG runs on Dirac_Wilson_evenodd")
+        self.M = op
+        self.accuracy = float(accuracy)
+        self.maxiters = int(maxiters)
+        self.precision = precision
+        self.true_residual = true_residual
+        self.delta = delta
+        self.use_graph = use_graph
+        self.last = None
+
+    def apply(self, inp: Field, out: Field) -> CGResult:
+        p = _params(self.accuracy, self.maxiters, self.precision, self.delta, self.true_residual, self.use_graph)
+        r = _CgResult()
+        rc = lib().hw_cg_solve(self.M.gauge.handle, self.M.kappa, inp.handle, out.handle, ctypes.byref(p),
+                               ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        self.last = CGResult.from_c(r)
+        return self.last

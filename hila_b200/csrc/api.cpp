@@ -1,0 +1,428 @@
+// C-ABI entry points: contexts, lattices, fields and the FP64 operators.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "hw_internal.h"
+
+namespace hw {
+
+static thread_local std::string g_err;
+
+void set_error(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+void clear_error() { g_err.clear(); }
+
+int DevBuf::alloc(size_t n) {
+    release();
+    if (n == 0) return HW_OK;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        set_error("cudaMalloc(%zu bytes) failed: %s", n, cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? HW_ERR_OOM : HW_ERR_CUDA;
+    }
+    bytes = n;
+    return HW_OK;
+}
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+static int alloc_half(HalfBuf &h, int stride) {
+    h.stride = stride;
+    return h.buf.alloc((size_t)12 * stride * sizeof(double2));
+}
+
+int ensure_workspace(hw_lattice *lat) {
+    if (!lat->ws) lat->ws.reset(new CgWorkspace());
+    CgWorkspace &w = *lat->ws;
+    if (w.allocated) return HW_OK;
+    int rc;
+    for (HalfBuf *h : {&w.r, &w.p, &w.Dp, &w.DDp, &w.src, &w.res, &w.t})
+        if ((rc = alloc_half(*h, lat->stride)) != HW_OK) return rc;
+    w.allocated = true;
+    return HW_OK;
+}
+
+int ensure_stage(hw_context *ctx, size_t bytes) {
+    if (ctx->stage.bytes >= bytes) return HW_OK;
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ctx->stage.alloc(bytes);
+}
+
+int ensure_reduction_capacity(hw_context *ctx, long nblocks) {
+    size_t need = (size_t)4 * (nblocks + 1);
+    if (ctx->red_capacity_doubles >= need) return HW_OK;
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    int rc = ctx->red_partials.alloc(need * sizeof(double));
+    if (rc != HW_OK) return rc;
+    ctx->red_capacity_doubles = need;
+    return HW_OK;
+}
+
+}  // namespace hw
+
+using namespace hw;
+
+extern "C" {
+
+int hw_api_version(void) { return HW_API_VERSION; }
+
+const char *hw_last_error(void) { return g_err.c_str(); }
+
+int hw_device_count(int *count) {
+    HW_CHECK_ARG(count, "count is null");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        set_error("cudaGetDeviceCount: %s", cudaGetErrorString(e));
+        return HW_ERR_NO_DEVICE;
+    }
+    *count = n;
+    return HW_OK;
+}
+
+int hw_context_create(int device, hw_context **out) {
+    HW_CHECK_ARG(out, "ctx out-pointer is null");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        set_error("no CUDA device available");
+        return HW_ERR_NO_DEVICE;
+    }
+    HW_CHECK_ARG(device >= 0 && device < n, "device %d out of range (%d devices)", device, n);
+    HW_CUDA(cudaSetDevice(device));
+    std::unique_ptr<hw_context> c(new hw_context());
+    c->device = device;
+    HW_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int rc;
+    if ((rc = c->red_ticket.alloc(64 * sizeof(unsigned))) != HW_OK) return rc;
+    HW_CUDA(cudaMemset(c->red_ticket.ptr, 0, 64 * sizeof(unsigned)));
+    if ((rc = ensure_reduction_capacity(c.get(), 1 << 16)) != HW_OK) return rc;
+    if ((rc = c->cg_state.alloc(sizeof(CgState))) != HW_OK) return rc;
+    HW_CUDA(cudaMemset(c->cg_state.ptr, 0, sizeof(CgState)));
+    HW_CUDA(cudaMallocHost(&c->cg_state_host, sizeof(CgState)));
+    HW_CUDA(cudaEventCreate(&c->ev0));
+    HW_CUDA(cudaEventCreate(&c->ev1));
+    *out = c.release();
+    clear_error();
+    return HW_OK;
+}
+
+int hw_context_destroy(hw_context *ctx) {
+    if (!ctx) return HW_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->cg_state_host) cudaFreeHost(ctx->cg_state_host);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    ctx->red_partials.release();
+    ctx->red_ticket.release();
+    ctx->cg_state.release();
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return HW_OK;
+}
+
+int hw_context_synchronize(hw_context *ctx) {
+    HW_CHECK_ARG(ctx, "ctx is null");
+    HW_CUDA(cudaSetDevice(ctx->device));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
+int hw_lattice_create(hw_context *ctx, const int dims[4], int t_antiperiodic, hw_lattice **out) {
+    HW_CHECK_ARG(ctx && dims && out, "null argument");
+    *out = nullptr;
+    long V = 1;
+    for (int d = 0; d < 4; d++) {
+        HW_CHECK_ARG(dims[d] >= 2 && dims[d] % 2 == 0, "dims[%d] = %d: every extent must be even and >= 2", d,
+                     dims[d]);
+        V *= dims[d];
+    }
+    HW_CHECK_ARG(V / 2 < (1L << 30), "lattice too large (%ld sites)", V);
+    std::unique_ptr<hw_lattice> l(new hw_lattice());
+    l->ctx = ctx;
+    for (int d = 0; d < 4; d++) l->dims[d] = dims[d];
+    l->tap = t_antiperiodic ? 1 : 0;
+    l->V = V;
+    l->Vh = V / 2;
+    l->stride = padded_stride(l->Vh);
+    Geom &g = l->g;
+    for (int d = 0; d < 4; d++) g.L[d] = dims[d];
+    g.lxh = dims[0] / 2;
+    g.Vh = (int)l->Vh;
+    g.sy = g.lxh;
+    g.sz = g.lxh * dims[1];
+    g.st = g.lxh * dims[1] * dims[2];
+    g.tap = l->tap;
+    *out = l.release();
+    clear_error();
+    return HW_OK;
+}
+
+int hw_lattice_destroy(hw_lattice *lat) {
+    if (!lat) return HW_OK;
+    cudaSetDevice(lat->ctx->device);
+    cudaStreamSynchronize(lat->ctx->stream);
+    delete lat;
+    return HW_OK;
+}
+
+int hw_lattice_volume(const hw_lattice *lat, int64_t *volume) {
+    HW_CHECK_ARG(lat && volume, "null argument");
+    *volume = lat->V;
+    return HW_OK;
+}
+
+int hw_gauge_create(hw_lattice *lat, const double *links, int link_format, hw_gauge **out) {
+    HW_CHECK_ARG(lat && links && out, "null argument");
+    HW_CHECK_ARG(link_format == 18 || link_format == 12, "link_format must be 18 or 12");
+    *out = nullptr;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    std::unique_ptr<hw_gauge> G(new hw_gauge());
+    G->lat = lat;
+    G->link_format = link_format;
+    const int planes = link_format == 12 ? 6 : 9;
+    int rc;
+    if ((rc = G->f64.alloc((size_t)8 * planes * lat->stride * sizeof(double2))) != HW_OK) return rc;
+    HW_CUDA(cudaMemsetAsync(G->f64.ptr, 0, G->f64.bytes, ctx->stream));
+    // stage one direction at a time: V links of 18 doubles
+    if ((rc = ensure_stage(ctx, (size_t)lat->V * 18 * sizeof(double))) != HW_OK) return rc;
+    DevBuf &stage = ctx->stage;
+    Geom g1 = lat->g;
+    for (int dir = 0; dir < 4; dir++) {
+        HW_CUDA(cudaMemcpyAsync(stage.ptr, links + (size_t)dir * lat->V * 18, (size_t)lat->V * 18 * sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        for (int par = 0; par < 2; par++) {
+            double2 *dst = G->f64.as<double2>() + (size_t)((par * 4 + dir) * planes) * lat->stride;
+            launch_links_lex_to_eo(g1, stage.as<double>(), dst, planes, lat->stride, par, ctx->stream);
+        }
+    }
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = G.release();
+    clear_error();
+    return HW_OK;
+}
+
+int hw_gauge_destroy(hw_gauge *gauge) {
+    if (!gauge) return HW_OK;
+    cudaSetDevice(gauge->lat->ctx->device);
+    cudaStreamSynchronize(gauge->lat->ctx->stream);
+    delete gauge;
+    return HW_OK;
+}
+
+int hw_field_create(hw_lattice *lat, hw_field **out) {
+    HW_CHECK_ARG(lat && out, "null argument");
+    *out = nullptr;
+    HW_CUDA(cudaSetDevice(lat->ctx->device));
+    std::unique_ptr<hw_field> f(new hw_field());
+    f->lat = lat;
+    int rc;
+    for (int p = 0; p < 2; p++) {
+        if ((rc = alloc_half(f->half[p], lat->stride)) != HW_OK) return rc;
+        HW_CUDA(cudaMemsetAsync(f->half[p].buf.ptr, 0, f->half[p].buf.bytes, lat->ctx->stream));
+    }
+    HW_CUDA(cudaStreamSynchronize(lat->ctx->stream));
+    *out = f.release();
+    clear_error();
+    return HW_OK;
+}
+
+int hw_field_destroy(hw_field *field) {
+    if (!field) return HW_OK;
+    cudaSetDevice(field->lat->ctx->device);
+    cudaStreamSynchronize(field->lat->ctx->stream);
+    delete field;
+    return HW_OK;
+}
+
+int hw_field_upload(hw_field *f, const double *host, int parity) {
+    HW_CHECK_ARG(f && host, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_lattice *lat = f->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)lat->V * 24 * sizeof(double);
+    int rc;
+    if ((rc = ensure_stage(ctx, bytes)) != HW_OK) return rc;
+    DevBuf &stage = ctx->stage;
+    HW_CUDA(cudaMemcpyAsync(stage.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) launch_spinor_lex_to_eo(lat->g, stage.as<double>(), p, f->half[p].h(), ctx->stream);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
+int hw_field_download(const hw_field *f, double *host, int parity) {
+    HW_CHECK_ARG(f && host, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_lattice *lat = f->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)lat->V * 24 * sizeof(double);
+    int rc;
+    if ((rc = ensure_stage(ctx, bytes)) != HW_OK) return rc;
+    DevBuf &stage = ctx->stage;
+    if (parity != 3) {
+        // keep the host's sites of the other parity: start from the host array
+        HW_CUDA(cudaMemcpyAsync(stage.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) launch_spinor_eo_to_lex(lat->g, f->half[p].h(), p, stage.as<double>(), ctx->stream);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaMemcpyAsync(host, stage.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
+int hw_field_zero(hw_field *f, int parity) {
+    HW_CHECK_ARG(f, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_context *ctx = f->lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) HW_CUDA(cudaMemsetAsync(f->half[p].buf.ptr, 0, f->half[p].buf.bytes, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
+// ------------------------------------------------------------------ operators
+
+static int check_op(const hw_gauge *g, const hw_field *in, const hw_field *out) {
+    HW_CHECK_ARG(g && in && out, "null argument");
+    HW_CHECK_ARG(in->lat == g->lat && out->lat == g->lat, "fields and gauge belong to different lattices");
+    return HW_OK;
+}
+
+static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_field *out, int sign) {
+    int rc = check_op(G, in, out);
+    if (rc != HW_OK) return rc;
+    hw_lattice *lat = G->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    if ((rc = ensure_workspace(lat)) != HW_OK) return rc;
+    CgWorkspace &w = *lat->ws;
+    // t_o = H^{oe}_s in_e ; out_e = in_e - kappa^2 H^{eo}_s t_o ; out_o = 0  (wilson.h:272-279)
+    launch_hop_scale(lat->g, G->U(), 1, sign, in->half[0].h(), w.t.h(), 1.0, nullptr, ctx->stream);
+    launch_hop_xpay(lat->g, G->U(), 0, sign, w.t.h(), in->half[0].h(), out->half[0].h(), -kappa * kappa, nullptr,
+                    nullptr, ctx->stream);
+    HW_CUDA(cudaMemsetAsync(out->half[1].buf.ptr, 0, out->half[1].buf.bytes, ctx->stream));
+    // stream-ordered: later calls on this context see the result; downloads synchronise
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+int hw_wilson_evenodd_apply(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out) {
+    return eo_apply(gauge, kappa, in, out, +1);
+}
+
+int hw_wilson_evenodd_dagger(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out) {
+    return eo_apply(gauge, kappa, in, out, -1);
+}
+
+int hw_wilson_apply(const hw_gauge *G, double kappa, int sign, const hw_field *in, hw_field *out) {
+    int rc = check_op(G, in, out);
+    if (rc != HW_OK) return rc;
+    HW_CHECK_ARG(sign == 1 || sign == -1, "sign must be +1 or -1");
+    HW_CHECK_ARG(in != out, "in and out must be different fields");
+    hw_lattice *lat = G->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    // out_p = in_p - kappa H_s in_{1-p} for both parities (wilson.h:183-192)
+    for (int p = 0; p < 2; p++)
+        launch_hop_xpay(lat->g, G->U(), p, sign, in->half[1 - p].h(), in->half[p].h(), out->half[p].h(), -kappa,
+                        nullptr, nullptr, ctx->stream);
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+int hw_wilson_hop(const hw_gauge *G, double kappa, const hw_field *in, hw_field *out, int parity, int sign, int set) {
+    int rc = check_op(G, in, out);
+    if (rc != HW_OK) return rc;
+    HW_CHECK_ARG(parity == HW_EVEN || parity == HW_ODD, "parity must be HW_EVEN or HW_ODD");
+    HW_CHECK_ARG(sign == 1 || sign == -1, "sign must be +1 or -1");
+    hw_lattice *lat = G->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    const int p = parity == HW_EVEN ? 0 : 1;
+    if (set)
+        launch_hop_scale(lat->g, G->U(), p, sign, in->half[1 - p].h(), out->half[p].h(), -kappa, nullptr,
+                         ctx->stream);
+    else
+        launch_hop_xpay(lat->g, G->U(), p, sign, in->half[1 - p].h(), out->half[p].h(), out->half[p].h(), -kappa,
+                        nullptr, nullptr, ctx->stream);
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+int hw_context_stream(hw_context *ctx, void **stream) {
+    HW_CHECK_ARG(ctx && stream, "null argument");
+    *stream = (void *)ctx->stream;
+    return HW_OK;
+}
+
+}  // extern "C"
+
+CgWorkspace::~CgWorkspace() {
+    if (init_exec) cudaGraphExecDestroy(init_exec);
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
+}
+
+hw_lattice::~hw_lattice() {
+    hw_field_destroy(host_b);
+    hw_field_destroy(host_x);
+}
+
+extern "C" {
+
+int hw_host_alloc(size_t bytes, void **ptr) {
+    HW_CHECK_ARG(ptr, "ptr is null");
+    *ptr = nullptr;
+    HW_CUDA(cudaMallocHost(ptr, bytes));
+    return HW_OK;
+}
+
+int hw_host_free(void *ptr) {
+    if (ptr) HW_CUDA(cudaFreeHost(ptr));
+    return HW_OK;
+}
+
+int hw_wilson_evenodd_solve_host(const hw_gauge *G, double kappa, const double *b_host, double *x_host,
+                                 const hw_cg_params *params, hw_cg_result *result) {
+    HW_CHECK_ARG(G && b_host && x_host, "null argument");
+    hw_lattice *lat = G->lat;
+    std::lock_guard<std::recursive_mutex> lk(lat->ctx->mu);
+    int rc;
+    if (!lat->host_b && (rc = hw_field_create(lat, &lat->host_b)) != HW_OK) return rc;
+    if (!lat->host_x && (rc = hw_field_create(lat, &lat->host_x)) != HW_OK) return rc;
+    if ((rc = hw_field_upload(lat->host_b, b_host, HW_EVEN)) != HW_OK) return rc;
+    if ((rc = hw_field_zero(lat->host_x, HW_ALL)) != HW_OK) return rc;
+    int st = hw_wilson_evenodd_solve(G, kappa, lat->host_b, lat->host_x, params, result);
+    if (st != HW_OK && st != HW_ERR_NOT_CONVERGED) return st;
+    if ((rc = hw_field_download(lat->host_x, x_host, HW_ALL)) != HW_OK) return rc;
+    return st;
+}
+
+}  // extern "C"

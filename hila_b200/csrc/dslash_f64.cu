@@ -1,0 +1,377 @@
+// FP64 even-odd Wilson hopping-term kernels with fused epilogues, and the
+// FP64 vector kernels of the conjugate gradient.
+//
+// One thread per output site over the SoA even-odd layout (storage.cuh).  The
+// hopping term follows libraries/dirac/wilson.h:15-95 (with the intended
+// backward gather vtemp[-dir][X-dir]); instead of the reference's eight
+// projection kernels, eight temporary half-spinor fields and four accumulate
+// kernels per hop, each output site gathers its eight neighbours, projects,
+// multiplies by the link and expands in registers, and the epilogue fuses
+// whatever the caller does next (scaling, the diagonal term of the even-odd
+// operator, the CG axpy updates and their dot products).
+#include "kernels.h"
+#include "reduce.cuh"
+#include "storage.cuh"
+
+namespace hw {
+
+namespace {
+
+__host__ __device__ __forceinline__ SpinorF64 sp(HalfF64 h) { return SpinorF64{h.p, h.stride}; }
+
+// out = a * H in
+struct EpiScale {
+    static constexpr int NRED = 0;
+    SpinorF64 out;
+    double a;
+    const CgState *st;
+    __device__ bool skip() const { return st && st->status != CG_RUNNING; }
+    __device__ void operator()(int i, Spinor<double> &acc, double *) const {
+#pragma unroll
+        for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = a * acc.s[c / 3][c % 3];
+        out.store(i, acc);
+    }
+    __device__ void operator()(const double *) {}
+};
+
+// out = x + b * H in ; optionally pAp = |out|^2 and alpha = rr / pAp
+template <bool RED>
+struct EpiXpay {
+    static constexpr int NRED = RED ? 1 : 0;
+    SpinorF64 x, out;
+    double b;
+    CgState *st;
+    __device__ bool skip() const { return st && st->status != CG_RUNNING; }
+    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+        Spinor<double> w;
+        x.load_cached(i, w);
+        double n2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<double> v = w.s[c / 3][c % 3] + b * acc.s[c / 3][c % 3];
+            acc.s[c / 3][c % 3] = v;
+            n2 += norm2(v);
+        }
+        out.store(i, acc);
+        if (RED) red[0] = n2;
+    }
+    __device__ void operator()(const double *tot) {
+        st->pAp = tot[0];
+        if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
+            st->status = CG_BREAKDOWN;
+            st->alpha = 0.0;
+        } else {
+            st->alpha = st->rr / tot[0];
+        }
+    }
+};
+
+// CG step fused into the second hop of M^dagger (conjugate_gradient.h:77-95):
+// DDp = Dp + b H t ; x += alpha p ; r -= alpha DDp ; rrnew = |r|^2
+struct EpiCgUpdate {
+    static constexpr int NRED = 1;
+    SpinorF64 Dp, r, x, p;
+    double b;
+    CgState *st;
+    __device__ bool skip() const { return st->status != CG_RUNNING; }
+    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+        const double alpha = st->alpha;
+        Spinor<double> w;
+        Dp.load_cached(i, w);
+        double n2 = 0;
+        Spinor<double> rr, xx, pp;
+        r.load_cached(i, rr);
+        x.load_cached(i, xx);
+        p.load_cached(i, pp);
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            const int s = c / 3, k = c % 3;
+            Cx<double> ddp = w.s[s][k] + b * acc.s[s][k];
+            rr.s[s][k] = rr.s[s][k] - alpha * ddp;
+            xx.s[s][k] = xx.s[s][k] + alpha * pp.s[s][k];
+            n2 += norm2(rr.s[s][k]);
+        }
+        r.store(i, rr);
+        x.store(i, xx);
+        red[0] = n2;
+    }
+    __device__ void operator()(const double *tot) {
+        const double rrnew = tot[0];
+        st->iter += 1;
+        if (!isfinite(rrnew)) {
+            st->status = CG_BREAKDOWN;
+        } else {
+            st->beta = rrnew / st->rr;
+            st->rr = rrnew;
+            if (rrnew < st->target_rr)
+                st->status = CG_CONVERGED;
+            else if (st->iter >= st->maxiter)
+                st->status = CG_MAXITER;
+        }
+        st->do_pupdate = st->status != CG_BREAKDOWN;
+    }
+};
+
+// res = src - (x + b H t) ; |res|^2, |src|^2
+struct EpiResidual {
+    static constexpr int NRED = 2;
+    SpinorF64 x, src, res;
+    double b;
+    CgState *st;
+    __device__ bool skip() const { return false; }
+    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+        Spinor<double> w, sv;
+        x.load_cached(i, w);
+        src.load_cached(i, sv);
+        double n2 = 0, d2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            const int s = c / 3, k = c % 3;
+            Cx<double> v = sv.s[s][k] - (w.s[s][k] + b * acc.s[s][k]);
+            acc.s[s][k] = v;
+            n2 += norm2(v);
+            d2 += norm2(sv.s[s][k]);
+        }
+        if (res.p) res.store(i, acc);
+        red[0] = n2;
+        red[1] = d2;
+    }
+    __device__ void operator()(const double *tot) {
+        st->res_num2 = tot[0];
+        st->res_den2 = tot[1];
+    }
+};
+
+template <int SIGN, class Lk, class Epi>
+__global__ void __launch_bounds__(kHopBlock) k_hop(Geom g, Lk U, int par, SpinorF64 in, Epi epi, RedBuf red) {
+    if (epi.skip()) return;
+    const int i = blockIdx.x * kHopBlock + threadIdx.x;
+    double v[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+    for (int k = 0; k < (Epi::NRED > 0 ? Epi::NRED : 1); k++) v[k] = 0.0;
+    if (i < g.Vh) {
+        Spinor<double> acc;
+        hop_site<SIGN>(g, par, i, in, U, acc);
+        epi(i, acc, v);
+    }
+    if constexpr (Epi::NRED > 0) grid_reduce<Epi::NRED, kHopBlock>(v, red.partials, red.ticket, epi);
+}
+
+template <class Epi>
+void dispatch_hop(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, const Epi &epi, const RedBuf *red,
+                  cudaStream_t s) {
+    dim3 grid((g.Vh + kHopBlock - 1) / kHopBlock);
+    RedBuf rb = red ? *red : RedBuf{nullptr, nullptr};
+    SpinorF64 sin{in.p, in.stride};
+    if (U.planes == 9) {
+        LinksF64x18 L{U.p, U.stride};
+        if (sign > 0)
+            k_hop<1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
+        else
+            k_hop<-1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
+    } else {
+        LinksF64x12 L{U.p, U.stride};
+        if (sign > 0)
+            k_hop<1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
+        else
+            k_hop<-1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
+    }
+}
+
+// ------------------------------------------------------------------ vectors
+
+constexpr int kVecBlock = 256;
+
+struct FinCgInit {
+    CgState *st;
+    double acc2;
+    int maxiter;
+    __device__ void operator()(const double *tot) {
+        st->rr = tot[0];
+        st->src_norm2 = tot[1];
+        st->target_rr = acc2 * tot[1];
+        st->iter = 0;
+        st->maxiter = maxiter;
+        st->alpha = st->beta = 0.0;
+        st->do_pupdate = 0;
+        if (!isfinite(tot[0]) || !isfinite(tot[1]))
+            st->status = CG_BREAKDOWN;
+        else if (tot[1] == 0.0 || tot[0] < st->target_rr)
+            st->status = CG_CONVERGED;
+        else
+            st->status = CG_RUNNING;
+    }
+};
+
+__global__ void __launch_bounds__(kVecBlock) k_cg_init(int Vh, SpinorF64 src, SpinorF64 Ax, int have_ax, SpinorF64 r,
+                                                       SpinorF64 p, FinCgInit fin, RedBuf red) {
+    const int i = blockIdx.x * kVecBlock + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < Vh) {
+        Spinor<double> b, a;
+        src.load_cached(i, b);
+        if (have_ax) Ax.load_cached(i, a);
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            const int s = c / 3, k = c % 3;
+            v[1] += norm2(b.s[s][k]);
+            if (have_ax) b.s[s][k] = b.s[s][k] - a.s[s][k];
+            v[0] += norm2(b.s[s][k]);
+        }
+        r.store(i, b);
+        p.store(i, b);
+    }
+    grid_reduce<2, kVecBlock>(v, red.partials, red.ticket, fin);
+}
+
+__global__ void __launch_bounds__(kVecBlock) k_cg_pupdate(int Vh, SpinorF64 r, SpinorF64 p, const CgState *st) {
+    if (!st->do_pupdate) return;
+    const int i = blockIdx.x * kVecBlock + threadIdx.x;
+    if (i >= Vh) return;
+    const double beta = st->beta;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+        double2 rv = r.p[(size_t)c * r.stride + i];
+        double2 pv = p.p[(size_t)c * p.stride + i];
+        p.p[(size_t)c * p.stride + i] = make_double2(fma(beta, pv.x, rv.x), fma(beta, pv.y, rv.y));
+    }
+}
+
+// Last node of every CG loop-body iteration: keeps the graph's while loop
+// going only while the solve is running.  It always runs, so the loop ends
+// even when every other body kernel returned early; the iteration counter is
+// bounded by maxiter, so the loop is bounded.
+__global__ void k_loop_control(CgState *st, cudaGraphConditionalHandle cond, int use_cond) {
+    st->do_pupdate = 0;
+    if (st->status == CG_RUNNING && st->iter >= st->maxiter) st->status = CG_MAXITER;
+    if (use_cond) cudaGraphSetConditional(cond, st->status == CG_RUNNING ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(kVecBlock) k_scale(int Vh, SpinorF64 x, SpinorF64 y, double a) {
+    const int i = blockIdx.x * kVecBlock + threadIdx.x;
+    if (i >= Vh) return;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+        double2 v = x.p[(size_t)c * x.stride + i];
+        y.p[(size_t)c * y.stride + i] = make_double2(a * v.x, a * v.y);
+    }
+}
+
+// ------------------------------------------------------------------ layout
+
+// lexicographic AoS [V][4][3] complex -> even-odd SoA half lattice of parity par
+__global__ void k_spinor_lex_to_eo(Geom g, const double2 *lex, int par, SpinorF64 out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.Vh) return;
+    const int xh = i % g.lxh;
+    int r = i / g.lxh;
+    const int y = r % g.L[1];
+    r /= g.L[1];
+    const int z = r % g.L[2];
+    const int t = r / g.L[2];
+    const int x = 2 * xh + ((y + z + t + par) & 1);
+    const size_t lexi = x + (size_t)g.L[0] * (y + (size_t)g.L[1] * (z + (size_t)g.L[2] * t));
+#pragma unroll
+    for (int c = 0; c < 12; c++) out.p[(size_t)c * out.stride + i] = lex[lexi * 12 + c];
+}
+
+__global__ void k_spinor_eo_to_lex(Geom g, SpinorF64 in, int par, double2 *lex) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.Vh) return;
+    const int xh = i % g.lxh;
+    int r = i / g.lxh;
+    const int y = r % g.L[1];
+    r /= g.L[1];
+    const int z = r % g.L[2];
+    const int t = r / g.L[2];
+    const int x = 2 * xh + ((y + z + t + par) & 1);
+    const size_t lexi = x + (size_t)g.L[0] * (y + (size_t)g.L[1] * (z + (size_t)g.L[2] * t));
+#pragma unroll
+    for (int c = 0; c < 12; c++) lex[lexi * 12 + c] = in.p[(size_t)c * in.stride + i];
+}
+
+// links of one direction, [V][3][3] complex lexicographic -> the `nplanes`
+// planes of (par, dir): dst[k*stride + i]
+__global__ void k_links_lex_to_eo(Geom g, const double2 *lex_dir, double2 *dst, int nplanes, int stride, int par) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.Vh) return;
+    const int xh = i % g.lxh;
+    int r = i / g.lxh;
+    const int y = r % g.L[1];
+    r /= g.L[1];
+    const int z = r % g.L[2];
+    const int t = r / g.L[2];
+    const int x = 2 * xh + ((y + z + t + par) & 1);
+    const size_t lexi = x + (size_t)g.L[0] * (y + (size_t)g.L[1] * (z + (size_t)g.L[2] * t));
+    const double2 *src = lex_dir + lexi * 9;
+    for (int k = 0; k < nplanes; k++) dst[(size_t)k * stride + i] = src[k];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+
+void launch_hop_scale(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 out, double a,
+                      const CgState *st, cudaStream_t s) {
+    EpiScale e{sp(out), a, st};
+    dispatch_hop(g, U, par, sign, in, e, nullptr, s);
+}
+
+void launch_hop_xpay(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 x, HalfF64 out,
+                     double b, CgState *st, const RedBuf *red, cudaStream_t s) {
+    if (red) {
+        EpiXpay<true> e{sp(x), sp(out), b, st};
+        dispatch_hop(g, U, par, sign, in, e, red, s);
+    } else {
+        EpiXpay<false> e{sp(x), sp(out), b, st};
+        dispatch_hop(g, U, par, sign, in, e, nullptr, s);
+    }
+}
+
+void launch_hop_cg_update(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 Dp, HalfF64 r,
+                          HalfF64 x, HalfF64 p, double b, CgState *st, const RedBuf &red,
+                          cudaStream_t s) {
+    EpiCgUpdate e{sp(Dp), sp(r), sp(x), sp(p), b, st};
+    dispatch_hop(g, U, par, sign, t, e, &red, s);
+}
+
+void launch_hop_residual(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 x, HalfF64 src,
+                         HalfF64 res, double b, CgState *st, const RedBuf &red, cudaStream_t s) {
+    EpiResidual e{sp(x), sp(src), sp(res), b, st};
+    dispatch_hop(g, U, par, sign, t, e, &red, s);
+}
+
+void launch_cg_init(int Vh, HalfF64 src, HalfF64 Ax, HalfF64 r, HalfF64 p, double acc2, int maxiter, CgState *st,
+                    const RedBuf &red, cudaStream_t s) {
+    FinCgInit fin{st, acc2, maxiter};
+    k_cg_init<<<(Vh + kVecBlock - 1) / kVecBlock, kVecBlock, 0, s>>>(Vh, sp(src), sp(Ax), Ax.p != nullptr, sp(r),
+                                                                      sp(p), fin, red);
+}
+
+void launch_cg_pupdate(int Vh, HalfF64 r, HalfF64 p, const CgState *st, cudaStream_t s) {
+    k_cg_pupdate<<<(Vh + kVecBlock - 1) / kVecBlock, kVecBlock, 0, s>>>(Vh, sp(r), sp(p), st);
+}
+
+void launch_loop_control(CgState *st, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t s) {
+    k_loop_control<<<1, 1, 0, s>>>(st, cond, use_cond);
+}
+
+void launch_scale(int Vh, HalfF64 x, HalfF64 y, double a, cudaStream_t s) {
+    k_scale<<<(Vh + kVecBlock - 1) / kVecBlock, kVecBlock, 0, s>>>(Vh, sp(x), sp(y), a);
+}
+
+void launch_spinor_lex_to_eo(const Geom &g, const double *lex, int par, HalfF64 out, cudaStream_t s) {
+    k_spinor_lex_to_eo<<<(g.Vh + 255) / 256, 256, 0, s>>>(g, reinterpret_cast<const double2 *>(lex), par, sp(out));
+}
+
+void launch_spinor_eo_to_lex(const Geom &g, HalfF64 in, int par, double *lex, cudaStream_t s) {
+    k_spinor_eo_to_lex<<<(g.Vh + 255) / 256, 256, 0, s>>>(g, sp(in), par, reinterpret_cast<double2 *>(lex));
+}
+
+void launch_links_lex_to_eo(const Geom &g, const double *lex_dir, double2 *dst, int nplanes, int stride, int par,
+                            cudaStream_t s) {
+    k_links_lex_to_eo<<<(g.Vh + 255) / 256, 256, 0, s>>>(g, reinterpret_cast<const double2 *>(lex_dir), dst, nplanes,
+                                                        stride, par);
+}
+
+}  // namespace hw

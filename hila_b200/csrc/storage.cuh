@@ -1,0 +1,257 @@
+// HBM storage formats for spinor and gauge fields, and their device accessors.
+//
+// All fields are stored per parity ("half-lattice arrays") in a
+// structure-of-arrays layout over checkerboard sites, so that a warp reading
+// one component for 32 consecutive sites issues one fully coalesced 512-byte
+// (FP64) or 256-byte request:
+//
+//   FP64 spinor   12 x double2 planes           component c at p[c*stride + i]
+//   FP32 spinor    6 x float4 planes            components 2k,2k+1 at p[k*stride + i]
+//   FP16 spinor    3 x uint4 planes + float     components 4k..4k+3 (8 halves) at
+//                  norm plane                   p[k*stride + i], scaled by norm[i]
+//
+//   FP64 links, 18 reals: 9 double2 planes per (parity, dir)
+//   FP64 links, 12 reals: 6 double2 planes (rows 0,1; row 2 rebuilt)
+//   FP32 links, 12 reals: 3 float4 planes
+//   FP16 links, 12 reals: 1 uint4 plane (elements 0..3) + 1 uint2 plane (4,5)
+//
+// Plane index for links: ((parity*4 + dir)*planes + k)*stride + i.
+// `stride` is the padded number of sites per parity (a multiple of 64).
+#pragma once
+
+#include "wilson_math.cuh"
+
+namespace hw {
+
+enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2 };
+
+// ------------------------------------------------------------------ spinors
+
+struct SpinorF64 {
+    using R = double;
+    double2 *p;
+    int stride;
+    __device__ __forceinline__ void load(int i, Spinor<double> &w) const {
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            double2 v = __ldg(p + (size_t)c * stride + i);
+            w.s[c / 3][c % 3] = {v.x, v.y};
+        }
+    }
+    __device__ __forceinline__ void load_cached(int i, Spinor<double> &w) const {
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            double2 v = p[(size_t)c * stride + i];
+            w.s[c / 3][c % 3] = {v.x, v.y};
+        }
+    }
+    __device__ __forceinline__ void store(int i, const Spinor<double> &w) const {
+#pragma unroll
+        for (int c = 0; c < 12; c++) p[(size_t)c * stride + i] = make_double2(w.s[c / 3][c % 3].re, w.s[c / 3][c % 3].im);
+    }
+};
+
+struct SpinorF32 {
+    using R = float;
+    float4 *p;
+    int stride;
+    __device__ __forceinline__ void load(int i, Spinor<float> &w) const {
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float4 v = __ldg(p + (size_t)k * stride + i);
+            int c0 = 2 * k, c1 = 2 * k + 1;
+            w.s[c0 / 3][c0 % 3] = {v.x, v.y};
+            w.s[c1 / 3][c1 % 3] = {v.z, v.w};
+        }
+    }
+    __device__ __forceinline__ void load_cached(int i, Spinor<float> &w) const { load(i, w); }
+    __device__ __forceinline__ void store(int i, const Spinor<float> &w) const {
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            int c0 = 2 * k, c1 = 2 * k + 1;
+            p[(size_t)k * stride + i] = make_float4(w.s[c0 / 3][c0 % 3].re, w.s[c0 / 3][c0 % 3].im,
+                                                    w.s[c1 / 3][c1 % 3].re, w.s[c1 / 3][c1 % 3].im);
+        }
+    }
+};
+
+// FP16 storage with a per-site scale: the 24 reals of a site are divided by
+// their largest magnitude (stored in norm[i]) before rounding to half, so
+// every stored value lies in [-1, 1].
+struct SpinorF16 {
+    using R = float;
+    uint4 *p;
+    float *norm;
+    int stride;
+    __device__ __forceinline__ void load(int i, Spinor<float> &w) const {
+        float nrm = __ldg(norm + i);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v = __ldg(p + (size_t)k * stride + i);
+            const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float2 f = __half22float2(h[q]);
+                int c = 4 * k + q;
+                w.s[c / 3][c % 3] = {f.x * nrm, f.y * nrm};
+            }
+        }
+    }
+    __device__ __forceinline__ void load_cached(int i, Spinor<float> &w) const { load(i, w); }
+    __device__ __forceinline__ void store(int i, const Spinor<float> &w) const {
+        float m = 0.f;
+#pragma unroll
+        for (int c = 0; c < 12; c++) m = fmaxf(m, fmaxf(fabsf(w.s[c / 3][c % 3].re), fabsf(w.s[c / 3][c % 3].im)));
+        float inv = m > 0.f ? 1.0f / m : 0.f;
+        norm[i] = m;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v;
+            __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                int c = 4 * k + q;
+                h[q] = __floats2half2_rn(w.s[c / 3][c % 3].re * inv, w.s[c / 3][c % 3].im * inv);
+            }
+            p[(size_t)k * stride + i] = v;
+        }
+    }
+};
+
+// ------------------------------------------------------------------ links
+
+struct LinksF64x18 {
+    using R = double;
+    static constexpr int planes = 9;
+    const double2 *p;
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<double> &u) const {
+        const double2 *b = p + (size_t)((par * 4 + dir) * 9) * stride + i;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            double2 v = __ldg(b + (size_t)k * stride);
+            u.e[k / 3][k % 3] = {v.x, v.y};
+        }
+    }
+};
+
+struct LinksF64x12 {
+    using R = double;
+    static constexpr int planes = 6;
+    const double2 *p;
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<double> &u) const {
+        const double2 *b = p + (size_t)((par * 4 + dir) * 6) * stride + i;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            double2 v = __ldg(b + (size_t)k * stride);
+            u.e[k / 3][k % 3] = {v.x, v.y};
+        }
+        reconstruct_row2(u);
+    }
+};
+
+struct LinksF32x12 {
+    using R = float;
+    static constexpr int planes = 3;
+    const float4 *p;
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
+        const float4 *b = p + (size_t)((par * 4 + dir) * 3) * stride + i;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float4 v = __ldg(b + (size_t)k * stride);
+            int e0 = 2 * k, e1 = 2 * k + 1;
+            u.e[e0 / 3][e0 % 3] = {v.x, v.y};
+            u.e[e1 / 3][e1 % 3] = {v.z, v.w};
+        }
+        reconstruct_row2(u);
+    }
+};
+
+// Link entries of an SU(3) matrix lie in [-1, 1]; FP16 stores them unscaled.
+struct LinksF16x12 {
+    using R = float;
+    const uint4 *p;   // elements 0..3 of rows 0,1 (per (parity, dir) plane)
+    const uint2 *q;   // elements 4..5
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
+        size_t o = (size_t)(par * 4 + dir) * stride + i;
+        uint4 a = __ldg(p + o);
+        uint2 b = __ldg(q + o);
+        const __half2 *ha = reinterpret_cast<const __half2 *>(&a);
+        const __half2 *hb = reinterpret_cast<const __half2 *>(&b);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float2 f = __half22float2(ha[k]);
+            u.e[k / 3][k % 3] = {f.x, f.y};
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            float2 f = __half22float2(hb[k]);
+            u.e[(k + 4) / 3][(k + 4) % 3] = {f.x, f.y};
+        }
+        reconstruct_row2(u);
+    }
+};
+
+// ------------------------------------------------------------------ hopping term
+//
+// acc = (H_s in)(x) for checkerboard site i of parity par (the output parity);
+// `in` holds the opposite parity.  Forward term uses U_mu(x) (parity par),
+// backward term U_mu(x-mu) (opposite parity, at the neighbour's index).
+
+template <int MU, int SIGN, class SpIn, class Lk, typename R>
+__device__ __forceinline__ void hop_dir(const SiteNbrs &n, int par, int i, const SpIn &in, const Lk &U,
+                                        Spinor<R> &acc) {
+    Cx<R> h0[3], h1[3], v0[3], v1[3];
+    Su3<R> u;
+    {
+        Spinor<R> w;
+        in.load(n.fwd[MU], w);
+        project<MU, SIGN>(w, h0, h1);
+        if (MU == 3) {
+            const R sg = n.tfwd_wrap ? R(-1) : R(1);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                h0[k] = sg * h0[k];
+                h1[k] = sg * h1[k];
+            }
+        }
+        U.load(par, MU, i, u);
+        su3_mul(u, h0, v0);
+        su3_mul(u, h1, v1);
+        expand_add<MU, SIGN>(acc, v0, v1);
+    }
+    {
+        Spinor<R> w;
+        in.load(n.bwd[MU], w);
+        project<MU, -SIGN>(w, h0, h1);
+        if (MU == 3) {
+            const R sg = n.tbwd_wrap ? R(-1) : R(1);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                h0[k] = sg * h0[k];
+                h1[k] = sg * h1[k];
+            }
+        }
+        U.load(1 - par, MU, n.bwd[MU], u);
+        su3_adj_mul(u, h0, v0);
+        su3_adj_mul(u, h1, v1);
+        expand_add<MU, -SIGN>(acc, v0, v1);
+    }
+}
+
+template <int SIGN, class SpIn, class Lk, typename R>
+__device__ __forceinline__ void hop_site(const Geom &g, int par, int i, const SpIn &in, const Lk &U,
+                                         Spinor<R> &acc) {
+#pragma unroll
+    for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {R(0), R(0)};
+    SiteNbrs n = site_neighbours(g, i, par);
+    hop_dir<0, SIGN>(n, par, i, in, U, acc);
+    hop_dir<1, SIGN>(n, par, i, in, U, acc);
+    hop_dir<2, SIGN>(n, par, i, in, U, acc);
+    hop_dir<3, SIGN>(n, par, i, in, U, acc);
+}
+
+}  // namespace hw

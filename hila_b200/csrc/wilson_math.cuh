@@ -1,0 +1,264 @@
+// Device-side site algebra for the Wilson even-odd operator on sm_100a.
+//
+// Complex arithmetic, SU(3) x colour-vector products, the half-spinor
+// projection P_{mu,s} and expansion E_{mu,s} of HILA's
+// libraries/datatypes/wilson_vector.h:439-567 (gamma basis :311-347), and the
+// even-odd site index arithmetic of libraries/plumbing/lattice.cpp:171-184.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hw {
+
+// ----------------------------------------------------------------- complex
+
+template <typename R>
+struct Cx {
+    R re, im;
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> cx(R a, R b) {
+    return Cx<R>{a, b};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator+(Cx<R> a, Cx<R> b) {
+    return {a.re + b.re, a.im + b.im};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(Cx<R> a, Cx<R> b) {
+    return {a.re - b.re, a.im - b.im};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(Cx<R> a) {
+    return {-a.re, -a.im};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator*(R s, Cx<R> a) {
+    return {s * a.re, s * a.im};
+}
+// i * a
+template <typename R>
+__device__ __forceinline__ Cx<R> mul_i(Cx<R> a) {
+    return {-a.im, a.re};
+}
+// a * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+// acc + a * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cmadd(Cx<R> acc, Cx<R> a, Cx<R> b) {
+    acc.re = fma(a.re, b.re, acc.re);
+    acc.re = fma(-a.im, b.im, acc.re);
+    acc.im = fma(a.re, b.im, acc.im);
+    acc.im = fma(a.im, b.re, acc.im);
+    return acc;
+}
+// acc + conj(a) * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cjmadd(Cx<R> acc, Cx<R> a, Cx<R> b) {
+    acc.re = fma(a.re, b.re, acc.re);
+    acc.re = fma(a.im, b.im, acc.re);
+    acc.im = fma(a.re, b.im, acc.im);
+    acc.im = fma(-a.im, b.re, acc.im);
+    return acc;
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> conj(Cx<R> a) {
+    return {a.re, -a.im};
+}
+template <typename R>
+__device__ __forceinline__ R norm2(Cx<R> a) {
+    return a.re * a.re + a.im * a.im;
+}
+
+// ----------------------------------------------------------------- SU(3)
+
+// 3x3 complex colour matrix, row-major.  Links may be stored with only their
+// first two rows; the third row of a special unitary matrix is
+// conj(row0 x row1).
+template <typename R>
+struct Su3 {
+    Cx<R> e[3][3];
+};
+
+template <typename R>
+__device__ __forceinline__ void reconstruct_row2(Su3<R> &u) {
+    // c_k = conj(a_i b_j - a_j b_i), (i,j,k) cyclic
+    const Cx<R> *a = u.e[0];
+    const Cx<R> *b = u.e[1];
+    u.e[2][0] = conj(cmul(a[1], b[2]) - cmul(a[2], b[1]));
+    u.e[2][1] = conj(cmul(a[2], b[0]) - cmul(a[0], b[2]));
+    u.e[2][2] = conj(cmul(a[0], b[1]) - cmul(a[1], b[0]));
+}
+
+// v = U h  (colour vector)
+template <typename R>
+__device__ __forceinline__ void su3_mul(const Su3<R> &u, const Cx<R> h[3], Cx<R> v[3]) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        Cx<R> a = cmul(u.e[i][0], h[0]);
+        a = cmadd(a, u.e[i][1], h[1]);
+        a = cmadd(a, u.e[i][2], h[2]);
+        v[i] = a;
+    }
+}
+// v = U^dagger h
+template <typename R>
+__device__ __forceinline__ void su3_adj_mul(const Su3<R> &u, const Cx<R> h[3], Cx<R> v[3]) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        Cx<R> a = {u.e[0][i].re * h[0].re + u.e[0][i].im * h[0].im,
+                   u.e[0][i].re * h[0].im - u.e[0][i].im * h[0].re};
+        a = cjmadd(a, u.e[1][i], h[1]);
+        a = cjmadd(a, u.e[2][i], h[2]);
+        v[i] = a;
+    }
+}
+
+// ----------------------------------------------------------------- spinors
+//
+// A Wilson spinor is 4 spins x 3 colours; component index c = 3*spin + colour.
+
+template <typename R>
+struct Spinor {
+    Cx<R> s[4][3];
+};
+
+// Half spinor h = P_{dir,sign} w, wilson_vector.h:439-491.
+template <int DIR, int SIGN, typename R>
+__device__ __forceinline__ void project(const Spinor<R> &w, Cx<R> h0[3], Cx<R> h1[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (DIR == 0) {  // x: w0 + s i w3, w1 + s i w2
+            if (SIGN > 0) {
+                h0[k] = w.s[0][k] + mul_i(w.s[3][k]);
+                h1[k] = w.s[1][k] + mul_i(w.s[2][k]);
+            } else {
+                h0[k] = w.s[0][k] - mul_i(w.s[3][k]);
+                h1[k] = w.s[1][k] - mul_i(w.s[2][k]);
+            }
+        } else if (DIR == 1) {  // y: w0 - s w3, w1 + s w2
+            if (SIGN > 0) {
+                h0[k] = w.s[0][k] - w.s[3][k];
+                h1[k] = w.s[1][k] + w.s[2][k];
+            } else {
+                h0[k] = w.s[0][k] + w.s[3][k];
+                h1[k] = w.s[1][k] - w.s[2][k];
+            }
+        } else if (DIR == 2) {  // z: w0 + s i w2, w1 - s i w3
+            if (SIGN > 0) {
+                h0[k] = w.s[0][k] + mul_i(w.s[2][k]);
+                h1[k] = w.s[1][k] - mul_i(w.s[3][k]);
+            } else {
+                h0[k] = w.s[0][k] - mul_i(w.s[2][k]);
+                h1[k] = w.s[1][k] + mul_i(w.s[3][k]);
+            }
+        } else {  // t: w0 + s w2, w1 + s w3
+            if (SIGN > 0) {
+                h0[k] = w.s[0][k] + w.s[2][k];
+                h1[k] = w.s[1][k] + w.s[3][k];
+            } else {
+                h0[k] = w.s[0][k] - w.s[2][k];
+                h1[k] = w.s[1][k] - w.s[3][k];
+            }
+        }
+    }
+}
+
+// acc += E_{dir,sign}(h) = (1 + sign gamma_dir) w, wilson_vector.h:493-567.
+template <int DIR, int SIGN, typename R>
+__device__ __forceinline__ void expand_add(Spinor<R> &acc, const Cx<R> h0[3], const Cx<R> h1[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        acc.s[0][k] = acc.s[0][k] + h0[k];
+        acc.s[1][k] = acc.s[1][k] + h1[k];
+        if (DIR == 0) {  // r2 = -s i h1, r3 = -s i h0
+            if (SIGN > 0) {
+                acc.s[2][k] = acc.s[2][k] - mul_i(h1[k]);
+                acc.s[3][k] = acc.s[3][k] - mul_i(h0[k]);
+            } else {
+                acc.s[2][k] = acc.s[2][k] + mul_i(h1[k]);
+                acc.s[3][k] = acc.s[3][k] + mul_i(h0[k]);
+            }
+        } else if (DIR == 1) {  // r2 = s h1, r3 = -s h0
+            if (SIGN > 0) {
+                acc.s[2][k] = acc.s[2][k] + h1[k];
+                acc.s[3][k] = acc.s[3][k] - h0[k];
+            } else {
+                acc.s[2][k] = acc.s[2][k] - h1[k];
+                acc.s[3][k] = acc.s[3][k] + h0[k];
+            }
+        } else if (DIR == 2) {  // r2 = -s i h0, r3 = s i h1
+            if (SIGN > 0) {
+                acc.s[2][k] = acc.s[2][k] - mul_i(h0[k]);
+                acc.s[3][k] = acc.s[3][k] + mul_i(h1[k]);
+            } else {
+                acc.s[2][k] = acc.s[2][k] + mul_i(h0[k]);
+                acc.s[3][k] = acc.s[3][k] - mul_i(h1[k]);
+            }
+        } else {  // r2 = s h0, r3 = s h1
+            if (SIGN > 0) {
+                acc.s[2][k] = acc.s[2][k] + h0[k];
+                acc.s[3][k] = acc.s[3][k] + h1[k];
+            } else {
+                acc.s[2][k] = acc.s[2][k] - h0[k];
+                acc.s[3][k] = acc.s[3][k] - h1[k];
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------- geometry
+//
+// Even-odd layout: a site with lexicographic index
+// lex = x + Lx*(y + Ly*(z + Lz*t)) and parity (x+y+z+t)&1 lives at
+// checkerboard index lex/2 inside the half-lattice array of its parity
+// (lattice.cpp:171-184 with even sites first).  Lx must be even.
+
+struct Geom {
+    int L[4];       // Lx, Ly, Lz, Lt
+    int lxh;        // Lx / 2
+    int Vh;         // sites per parity
+    int sy, sz, st; // checkerboard strides of y, z, t: lxh, lxh*Ly, lxh*Ly*Lz
+    int tap;        // 1: fermion values crossing the t boundary are negated
+};
+
+struct SiteNbrs {
+    int fwd[4], bwd[4];  // checkerboard index of x+mu, x-mu (opposite parity)
+    bool tfwd_wrap, tbwd_wrap;
+};
+
+// neighbours of checkerboard site i of parity par
+__device__ __forceinline__ SiteNbrs site_neighbours(const Geom &g, int i, int par) {
+    SiteNbrs n;
+    int xh = i % g.lxh;
+    int r = i / g.lxh;
+    int y = r % g.L[1];
+    r /= g.L[1];
+    int z = r % g.L[2];
+    int t = r / g.L[2];
+    int x = 2 * xh + ((y + z + t + par) & 1);
+    int base = i - xh;
+    int xp = (x + 1 == g.L[0]) ? 0 : x + 1;
+    int xm = (x == 0) ? g.L[0] - 1 : x - 1;
+    n.fwd[0] = base + (xp >> 1);
+    n.bwd[0] = base + (xm >> 1);
+    n.fwd[1] = (y + 1 == g.L[1]) ? i - (g.L[1] - 1) * g.sy : i + g.sy;
+    n.bwd[1] = (y == 0) ? i + (g.L[1] - 1) * g.sy : i - g.sy;
+    n.fwd[2] = (z + 1 == g.L[2]) ? i - (g.L[2] - 1) * g.sz : i + g.sz;
+    n.bwd[2] = (z == 0) ? i + (g.L[2] - 1) * g.sz : i - g.sz;
+    n.tfwd_wrap = (t + 1 == g.L[3]);
+    n.tbwd_wrap = (t == 0);
+    n.fwd[3] = n.tfwd_wrap ? i - (g.L[3] - 1) * g.st : i + g.st;
+    n.bwd[3] = n.tbwd_wrap ? i + (g.L[3] - 1) * g.st : i - g.st;
+    n.tfwd_wrap = n.tfwd_wrap && g.tap;
+    n.tbwd_wrap = n.tbwd_wrap && g.tap;
+    return n;
+}
+
+}  // namespace hw

@@ -1,0 +1,195 @@
+/* hila_b200 — C ABI of the B200 Wilson-fermion solve path.
+ *
+ * Drop-in boundary for HILA's even-odd preconditioned Wilson operator and its
+ * conjugate-gradient inverter.  HILA exposes these as C++ templates
+ * (libraries/dirac/wilson.h, libraries/dirac/conjugate_gradient.h); every
+ * entry point below names the reference interface it replaces.  The
+ * C++ facade in include/hila_b200/wilson.hpp re-creates the reference's class
+ * signatures on top of this ABI.
+ *
+ * Conventions
+ *   - Every function returns an int status: HW_OK (0) or a negative HW_ERR_*
+ *     code; hw_last_error() gives a message for the calling thread.
+ *   - Host arrays use HILA's canonical site order: lexicographic index
+ *     x + Lx*(y + Ly*(z + Lz*t)) (libraries/plumbing/lattice.cpp:559-565).
+ *       spinor field: double[V][4 spin][3 colour][2]   (re, im)
+ *       gauge field:  double[4 dir][V][3][3][2]       (row-major SU(3) links)
+ *   - Parity masks follow HILA's Parity enum (plumbing/coordinates.h:182):
+ *     HW_EVEN = 1, HW_ODD = 2, HW_ALL = 3.
+ *   - Directions 0..3 = x, y, z, t.  Spinor fields are antiperiodic in t when
+ *     the lattice was created with t_antiperiodic = 1 (the reference sets
+ *     this per Field with set_boundary_condition(e_t, ANTIPERIODIC),
+ *     applications/test_cases/test_CG.cpp:222-226); links are periodic.
+ *   - Calls on one context are serialised by the context; different contexts
+ *     may be used from different threads.
+ */
+#ifndef HILA_B200_H
+#define HILA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HW_API_VERSION 1
+
+enum hw_status {
+    HW_OK = 0,
+    HW_ERR_INVALID = -1,       /* bad argument, size or handle */
+    HW_ERR_OOM = -2,           /* device allocation failed */
+    HW_ERR_CUDA = -3,          /* a CUDA call failed */
+    HW_ERR_NOT_CONVERGED = -4, /* solve hit maxiter above tolerance */
+    HW_ERR_BREAKDOWN = -5,     /* CG breakdown: p.Ap <= 0 or non-finite */
+    HW_ERR_TIMEOUT = -6,       /* a bounded device wait gave up */
+    HW_ERR_REJECTED = -7,      /* admission refused (over the memory budget) */
+    HW_ERR_CANCELLED = -8,     /* request cancelled before completion */
+    HW_ERR_NO_DEVICE = -9      /* no CUDA device / driver */
+};
+
+enum hw_parity { HW_EVEN = 1, HW_ODD = 2, HW_ALL = 3 };
+
+/* storage precision of spinors and links */
+enum hw_precision { HW_PREC_F64 = 0, HW_PREC_F32 = 1, HW_PREC_F16 = 2 };
+
+/* link storage of the FP64 operator: 18 reals, or 12 reals with the third
+ * row rebuilt as conj(row0 x row1) inside the kernel */
+enum hw_link_format { HW_LINKS_18 = 18, HW_LINKS_12 = 12 };
+
+typedef struct hw_context hw_context;
+typedef struct hw_lattice hw_lattice;
+typedef struct hw_gauge hw_gauge;
+typedef struct hw_field hw_field;
+
+/* ------------------------------------------------------------------ basics */
+
+int hw_api_version(void);
+/* message of the last failed call on this thread ("" if none) */
+const char *hw_last_error(void);
+int hw_device_count(int *count);
+
+/* One context per GPU: owns the stream, reduction buffers and graph caches.
+ * Replaces hila::initialize's device setup (libraries/plumbing/initialize.cpp). */
+int hw_context_create(int device, hw_context **ctx);
+int hw_context_destroy(hw_context *ctx);
+int hw_context_synchronize(hw_context *ctx);
+/* The context's CUDA stream (a cudaStream_t), so callers can order their own
+ * work or CUDA events with the library's.  Operator calls are stream-ordered:
+ * they return once the work is enqueued; downloads and solves synchronise. */
+int hw_context_stream(hw_context *ctx, void **stream);
+
+/* Page-locked host memory for fast host<->device transfers of field arrays
+ * (no reference counterpart; HILA allocates host memory with malloc). */
+int hw_host_alloc(size_t bytes, void **ptr);
+int hw_host_free(void *ptr);
+
+/* Lattice geometry (lattice.setup(size), plumbing/lattice.cpp:37-104).
+ * dims[0] (Lx) must be even; all dims >= 2 and even (even-odd split). */
+int hw_lattice_create(hw_context *ctx, const int dims[4], int t_antiperiodic, hw_lattice **lat);
+int hw_lattice_destroy(hw_lattice *lat);
+int hw_lattice_volume(const hw_lattice *lat, int64_t *volume);
+
+/* ------------------------------------------------------------------ fields */
+
+/* Gauge field Field<SU<3,double>> U[NDIM] (the operator holds it by
+ * reference, libraries/dirac/wilson.h:237, :261).  Uploads the host links once;
+ * link_format selects 18- or 12-real FP64 storage for the FP64 operator.
+ * Single- and half-precision copies for mixed-precision solves are made on
+ * first use. */
+int hw_gauge_create(hw_lattice *lat, const double *links, int link_format, hw_gauge **gauge);
+int hw_gauge_destroy(hw_gauge *gauge);
+
+/* FP64 Wilson spinor field, Field<Wilson_vector<3,double>> (full lattice,
+ * device resident, even-odd structure-of-arrays inside). */
+int hw_field_create(hw_lattice *lat, hw_field **field);
+int hw_field_destroy(hw_field *field);
+/* copy sites of `parity` from/to a host array in the canonical layout */
+int hw_field_upload(hw_field *field, const double *host, int parity);
+int hw_field_download(const hw_field *field, double *host, int parity);
+/* field[parity] = 0 */
+int hw_field_zero(hw_field *field, int parity);
+
+/* ------------------------------------------------------------------ operators */
+
+/* Dirac_Wilson_evenodd<SU<3,double>>::apply(in, out), wilson.h:272-279:
+ * out[EVEN] = in_e - kappa^2 H^{eo} H^{oe} in_e, out[ODD] = 0. */
+int hw_wilson_evenodd_apply(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out);
+/* Dirac_Wilson_evenodd::dagger(in, out), wilson.h:282-289 (sign -1) */
+int hw_wilson_evenodd_dagger(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out);
+
+/* Dirac_Wilson<SU<3,double>>::apply / dagger, wilson.h:183-192:
+ * out = in - kappa H_s in over ALL sites (sign +1 apply, -1 dagger). */
+int hw_wilson_apply(const hw_gauge *gauge, double kappa, int sign, const hw_field *in, hw_field *out);
+
+/* Dirac_Wilson_hop_set (set = 1: out[parity] = -kappa H_s in) and
+ * Dirac_Wilson_hop (set = 0: out[parity] -= kappa H_s in), wilson.h:15-95,
+ * with the backward term gathered from x - mu.  parity is HW_EVEN or HW_ODD. */
+int hw_wilson_hop(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out, int parity, int sign,
+                  int set);
+
+/* ------------------------------------------------------------------ solver */
+
+typedef struct hw_cg_params {
+    double accuracy;     /* relative accuracy (CG_DEFAULT_ACCURACY = 1e-12, conjugate_gradient.h:16) */
+    int maxiters;        /* CG_DEFAULT_MAXITERS = 10000 (conjugate_gradient.h:15) */
+    int precision;       /* HW_PREC_F64: plain FP64 CG; HW_PREC_F32 / HW_PREC_F16: mixed precision
+                            with FP64 reliable updates, solution accumulation and dot products */
+    double delta;        /* reliable-update trigger: recompute the FP64 residual when the iterated
+                            residual fell by this factor (mixed precision only; 0 = default 0.1) */
+    int true_residual;   /* 1: stop only when the explicitly recomputed FP64 residual meets
+                            accuracy; 0: reference stopping rule on the iterated residual */
+    int use_graph;       /* 1: device-resident iteration in a CUDA graph (default); 0: host loop */
+} hw_cg_params;
+
+typedef struct hw_cg_result {
+    int status;             /* HW_OK, HW_ERR_NOT_CONVERGED or HW_ERR_BREAKDOWN */
+    int iterations;         /* CG iterations (inner iterations in mixed precision) */
+    int reliable_updates;   /* FP64 residual recomputations */
+    int restarts;           /* continuations after an explicit residual check */
+    double rr_relative;     /* |r|^2/|in|^2 of the iterated residual, as the reference prints
+                               it (conjugate_gradient.h:103) */
+    double true_residual;   /* |b - A x| / |b| recomputed in FP64 */
+    double seconds;         /* device time of the solve */
+    int kernel_launches;    /* CUDA kernels the solve launched (graph nodes included) */
+} hw_cg_result;
+
+/* fill params with the reference defaults (accuracy 1e-12, maxiters 10000, FP64) */
+void hw_cg_params_default(hw_cg_params *params);
+
+/* CG<Dirac_Wilson_evenodd<SU<3,double>>>::apply(in, out),
+ * conjugate_gradient.h:46-104: solves (M^dagger M) out = in on EVEN sites;
+ * `out` holds the initial guess on entry. */
+int hw_cg_solve(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out,
+                const hw_cg_params *params, hw_cg_result *result);
+
+/* Solve M x = b on EVEN sites (M = Dirac_Wilson_evenodd) by CG on the normal
+ * equations with source M^dagger b — the D (D^dag D)^{-1} D^dag pattern of
+ * test_CG.cpp:254-256.  result->true_residual = |b - M x| / |b|; with
+ * params->true_residual = 1 the solve continues until that is <= accuracy. */
+int hw_wilson_evenodd_solve(const hw_gauge *gauge, double kappa, const hw_field *b, hw_field *x,
+                            const hw_cg_params *params, hw_cg_result *result);
+
+/* Same solve from and to host arrays (canonical layout, EVEN sites used):
+ * uploads b, solves, downloads x.  Host-to-device and device-to-host copies
+ * are part of the call. */
+int hw_wilson_evenodd_solve_host(const hw_gauge *gauge, double kappa, const double *b_host, double *x_host,
+                                 const hw_cg_params *params, hw_cg_result *result);
+
+/* ------------------------------------------------------------------ inputs */
+
+/* Seeded synthetic inputs (no reference counterpart beyond hila::seed_random
+ * + SU::random / gaussian_random; plumbing/random.cpp:60-70,187-199,
+ * datatypes/sun_matrix.h:137-196,480-560, matrix.h:3289-3309):
+ *   links  U = reunitarize(exp(eps * A)), A anti-Hermitian traceless from
+ *          8 Gaussian algebra coefficients of variance 2 per link
+ *   spinor every complex entry from Box-Muller (re, im each N(0,1)) on the
+ *          sites of parity_mask, zero elsewhere. */
+int hw_generate_links(const int dims[4], double eps, uint64_t seed, double *links);
+int hw_generate_spinor(const int dims[4], uint64_t seed, int parity_mask, double *spinor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HILA_B200_H */

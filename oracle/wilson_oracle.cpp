@@ -1,0 +1,815 @@
+// CPU oracle for the Wilson even-odd solve path — TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, in plain C++ on the host, the arithmetic of HILA's
+// Wilson-fermion path so that the CUDA library can be checked against it.
+// Only the test suite, the smoke check and the CPU-baseline leg of the bench
+// load it; the product library never links or calls it.
+//
+// Reference semantics followed (paths relative to the HILA source tree):
+//   * site order, parity, even-first index   libraries/plumbing/lattice.cpp:171-184, 559-574
+//   * gamma basis                             libraries/datatypes/wilson_vector.h:23, 311-347
+//   * half-spinor projection / expansion      libraries/datatypes/wilson_vector.h:439-567
+//   * hopping term (intended backward hop:
+//     vtemp[-dir][X-dir], see note below)     libraries/dirac/wilson.h:15-95
+//   * diag / diag_inverse                     libraries/dirac/wilson.h:98-106
+//   * unpreconditioned D = 1 - kappa H        libraries/dirac/wilson.h:183-192
+//   * even-odd apply / dagger                 libraries/dirac/wilson.h:272-289
+//   * conjugate gradient on M^dagger M        libraries/dirac/conjugate_gradient.h:46-104
+//   * antiperiodic fermion boundary in t      libraries/plumbing/field_comm.h:28-41 (negated gathers)
+//   * RNG: mt19937_64 + 9000 warm-up draws,
+//     uniform [0,1), Box-Muller gaussrand2    libraries/plumbing/random.cpp:60-70, 187-199
+//   * Complex::gaussian_random                libraries/datatypes/cmplx.h:344-349
+//   * su(3) algebra gaussian + expand         libraries/datatypes/sun_matrix.h:480-560
+//   * exp() Taylor order 20 (Horner)          libraries/datatypes/matrix.h:3289-3309
+//   * reunitarize = make_unitary + fix_det    libraries/datatypes/sun_matrix.h:137-196
+//
+// Backward hop.  wilson.h:47 (and :92) read vtemp[dir][X + dir] for the
+// backward term, although the U^dagger-multiplied half spinors are stored in
+// vtemp[-dir] and gathered from -dir (wilson.h:31,39,69,77).  As written apply
+// and dagger are not adjoint, which the reference's own test
+// (applications/test_cases/test_CG.cpp:236-245) asserts they are.  The oracle
+// implements the intended term  E_{mu,-s}( U_mu(x-mu)^dagger P_{mu,-s} psi(x-mu) ).
+//
+// Parity of this oracle is pinned by the reference's own identity tests
+// (test_CG.cpp: gamma identities, adjointness, CG identities) re-run on random
+// links, by an independent numpy restatement with explicit 4x4 gamma matrices,
+// and by the analytic free-field plane-wave spectrum.  The reference itself
+// cannot be compiled here (hilapp needs LLVM/Clang, MPI headers are absent and
+// the Wilson headers are bit-rotted) and ships no golden vectors for this path.
+//
+// Host data layouts (the canonical exchange layout of the C ABI as well):
+//   spinor field : psi[V][4 spin][3 colour] complex double, lexicographic
+//                  site index x + Lx*(y + Ly*(z + Lz*t)), 24 doubles per site
+//   gauge field  : U[4 dir][V][3][3] complex double, row-major, 18 doubles
+//                  per link; dir 0..3 = x,y,z,t
+
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using cd = std::complex<double>;
+const cd I1(0.0, 1.0);
+
+struct Geom {
+    int L[4];
+    long V, Vh;
+    int tap;  // antiperiodic fermion boundary in t
+
+    Geom(const int *dims, int antiperiodic) {
+        V = 1;
+        for (int d = 0; d < 4; d++) {
+            L[d] = dims[d];
+            V *= dims[d];
+        }
+        Vh = V / 2;
+        tap = antiperiodic;
+    }
+    void coords(long i, int c[4]) const {
+        for (int d = 0; d < 4; d++) {
+            c[d] = (int)(i % L[d]);
+            i /= L[d];
+        }
+    }
+    long lex(const int c[4]) const {
+        return c[0] + (long)L[0] * (c[1] + (long)L[1] * (c[2] + (long)L[2] * c[3]));
+    }
+    // neighbour of site i in direction dir (0..3), step +1 or -1; *sgn = -1
+    // when a fermion value crossing the t boundary must be negated.
+    long nb(long i, int dir, int step, double *sgn) const {
+        int c[4];
+        coords(i, c);
+        *sgn = 1.0;
+        c[dir] += step;
+        if (c[dir] == L[dir]) {
+            c[dir] = 0;
+            if (dir == 3 && tap) *sgn = -1.0;
+        } else if (c[dir] < 0) {
+            c[dir] = L[dir] - 1;
+            if (dir == 3 && tap) *sgn = -1.0;
+        }
+        return lex(c);
+    }
+    int parity(long i) const {
+        int c[4];
+        coords(i, c);
+        return (c[0] + c[1] + c[2] + c[3]) & 1;
+    }
+    // HILA Parity: EVEN=1, ODD=2, ALL=3 (plumbing/coordinates.h:182)
+    bool in(long i, int par) const {
+        int p = parity(i);
+        return (par & (p == 0 ? 1 : 2)) != 0;
+    }
+};
+
+struct Spinor {
+    cd s[4][3];
+};
+struct Half {
+    cd c[2][3];
+};
+struct Mat3 {
+    cd e[3][3];
+};
+
+inline Spinor load_spinor(const double *psi, long i) {
+    Spinor w;
+    const double *p = psi + 24 * i;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 3; b++) w.s[a][b] = cd(p[(a * 3 + b) * 2], p[(a * 3 + b) * 2 + 1]);
+    return w;
+}
+inline void store_spinor(double *psi, long i, const Spinor &w) {
+    double *p = psi + 24 * i;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 3; b++) {
+            p[(a * 3 + b) * 2] = w.s[a][b].real();
+            p[(a * 3 + b) * 2 + 1] = w.s[a][b].imag();
+        }
+}
+inline Mat3 load_link(const double *U, long V, int dir, long i) {
+    Mat3 m;
+    const double *p = U + 18 * (dir * V + i);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) m.e[a][b] = cd(p[(a * 3 + b) * 2], p[(a * 3 + b) * 2 + 1]);
+    return m;
+}
+
+// projection table, wilson_vector.h:439-491
+inline Half project(const Spinor &w, int dir, int sign) {
+    Half h;
+    const double s = sign;
+    for (int k = 0; k < 3; k++) {
+        switch (dir) {
+        case 0:  // x
+            h.c[0][k] = w.s[0][k] + s * I1 * w.s[3][k];
+            h.c[1][k] = w.s[1][k] + s * I1 * w.s[2][k];
+            break;
+        case 1:  // y
+            h.c[0][k] = w.s[0][k] - s * w.s[3][k];
+            h.c[1][k] = w.s[1][k] + s * w.s[2][k];
+            break;
+        case 2:  // z
+            h.c[0][k] = w.s[0][k] + s * I1 * w.s[2][k];
+            h.c[1][k] = w.s[1][k] - s * I1 * w.s[3][k];
+            break;
+        default:  // t
+            h.c[0][k] = w.s[0][k] + s * w.s[2][k];
+            h.c[1][k] = w.s[1][k] + s * w.s[3][k];
+            break;
+        }
+    }
+    return h;
+}
+
+// expansion table, wilson_vector.h:493-567:  E_{dir,sign}(h) = (1 + sign*gamma_dir) w
+inline Spinor expand(const Half &h, int dir, int sign) {
+    Spinor r;
+    const double s = sign;
+    for (int k = 0; k < 3; k++) {
+        r.s[0][k] = h.c[0][k];
+        r.s[1][k] = h.c[1][k];
+        switch (dir) {
+        case 0:
+            r.s[2][k] = -s * I1 * h.c[1][k];
+            r.s[3][k] = -s * I1 * h.c[0][k];
+            break;
+        case 1:
+            r.s[2][k] = s * h.c[1][k];
+            r.s[3][k] = -s * h.c[0][k];
+            break;
+        case 2:
+            r.s[2][k] = -s * I1 * h.c[0][k];
+            r.s[3][k] = s * I1 * h.c[1][k];
+            break;
+        default:
+            r.s[2][k] = s * h.c[0][k];
+            r.s[3][k] = s * h.c[1][k];
+            break;
+        }
+    }
+    return r;
+}
+
+inline Half mul(const Mat3 &U, const Half &h) {
+    Half r;
+    for (int a = 0; a < 2; a++)
+        for (int i = 0; i < 3; i++) {
+            cd acc = 0;
+            for (int j = 0; j < 3; j++) acc += U.e[i][j] * h.c[a][j];
+            r.c[a][i] = acc;
+        }
+    return r;
+}
+inline Half mul_adj(const Mat3 &U, const Half &h) {
+    Half r;
+    for (int a = 0; a < 2; a++)
+        for (int i = 0; i < 3; i++) {
+            cd acc = 0;
+            for (int j = 0; j < 3; j++) acc += std::conj(U.e[j][i]) * h.c[a][j];
+            r.c[a][i] = acc;
+        }
+    return r;
+}
+
+// (H_s psi)(x) = sum_mu E_{mu,s}(U_mu(x) P_{mu,s} psi(x+mu))
+//              + E_{mu,-s}(U_mu(x-mu)^dagger P_{mu,-s} psi(x-mu))
+// wilson.h:15-50 with the intended backward gather.
+inline Spinor hop_site(const Geom &g, const double *U, const double *in, long x, int sign) {
+    Spinor acc;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 3; b++) acc.s[a][b] = 0;
+    for (int mu = 0; mu < 4; mu++) {
+        double sf, sb;
+        long yf = g.nb(x, mu, +1, &sf);
+        long yb = g.nb(x, mu, -1, &sb);
+        Spinor wf = load_spinor(in, yf);
+        Spinor wb = load_spinor(in, yb);
+        Half hf = project(wf, mu, sign);
+        Half hb = project(wb, mu, -sign);
+        Spinor ef = expand(mul(load_link(U, g.V, mu, x), hf), mu, sign);
+        Spinor eb = expand(mul_adj(load_link(U, g.V, mu, yb), hb), mu, -sign);
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 3; b++) acc.s[a][b] += sf * ef.s[a][b] + sb * eb.s[a][b];
+    }
+    return acc;
+}
+
+// ---------------------------------------------------------------- RNG
+// random.cpp:60-70 (seed, 9000 warm-up), :187-199 (gaussrand2, variance 1)
+struct HostRng {
+    std::mt19937_64 gen;
+    std::uniform_real_distribution<double> uni{0.0, 1.0};
+    explicit HostRng(uint64_t seed) {
+        gen.seed(seed);
+        for (int i = 0; i < 9000; i++) gen();
+    }
+    double random() { return uni(gen); }
+    double gaussrand2(double &out2) {
+        double phi = 2.0 * M_PI * random();
+        double urnd;
+        do {
+            urnd = 1.0 - random();
+        } while (urnd == 0.0);
+        double r = std::sqrt(-std::log(urnd) * 2.0);
+        out2 = r * std::cos(phi);
+        return r * std::sin(phi);
+    }
+};
+
+// su(3) algebra element with coefficients a[8] -> anti-Hermitian traceless
+// matrix, sun_matrix.h:480-510 (expand).  Diagonal generators first, then the
+// off-diagonal pairs (0,1),(0,2),(1,2) as (re,im) coefficient pairs.
+Mat3 algebra_expand(const double a[8]) {
+    Mat3 m;
+    double d[3] = {0, 0, 0};
+    for (int i = 1; i < 3; i++) {
+        double r = a[i - 1] * std::sqrt(0.5 / (i * (i + 1)));
+        for (int j = 0; j < i; j++) d[j] += r;
+        d[i] = -i * r;
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m.e[i][j] = 0;
+    for (int i = 0; i < 3; i++) m.e[i][i] = cd(0, d[i]);
+    int k = 2;
+    for (int i = 0; i < 2; i++)
+        for (int j = i + 1; j < 3; j++) {
+            cd v(a[k] * 0.5, a[k + 1] * 0.5);
+            m.e[i][j] = v;
+            m.e[j][i] = -std::conj(v);
+            k += 2;
+        }
+    return m;
+}
+
+Mat3 matmul(const Mat3 &A, const Mat3 &B) {
+    Mat3 C;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            cd acc = 0;
+            for (int k = 0; k < 3; k++) acc += A.e[i][k] * B.e[k][j];
+            C.e[i][j] = acc;
+        }
+    return C;
+}
+
+// exp() by Horner-form Taylor series, order 20 (matrix.h:3289-3309)
+Mat3 mexp(const Mat3 &A) {
+    Mat3 r = A;
+    for (int k = 20; k > 1; k--) {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) r.e[i][j] *= (1.0 / k);
+        for (int i = 0; i < 3; i++) r.e[i][i] += 1.0;
+        r = matmul(r, A);
+    }
+    for (int i = 0; i < 3; i++) r.e[i][i] += 1.0;
+    return r;
+}
+
+cd det3(const Mat3 &m) {
+    return m.e[0][0] * (m.e[1][1] * m.e[2][2] - m.e[1][2] * m.e[2][1]) -
+           m.e[0][1] * (m.e[1][0] * m.e[2][2] - m.e[1][2] * m.e[2][0]) +
+           m.e[0][2] * (m.e[1][0] * m.e[2][1] - m.e[1][1] * m.e[2][0]);
+}
+
+// make_unitary + fix_det, sun_matrix.h:137-196
+void reunitarize(Mat3 &m) {
+    for (int r = 0; r < 3; r++) {
+        double n2 = 0;
+        for (int i = 0; i < 3; i++) n2 += std::norm(m.e[r][i]);
+        n2 = 1.0 / std::sqrt(n2);
+        for (int i = 0; i < 3; i++) m.e[r][i] *= n2;
+        for (int j = r + 1; j < 3; j++) {
+            cd d = 0;
+            for (int i = 0; i < 3; i++) d += std::conj(m.e[r][i]) * m.e[j][i];
+            for (int i = 0; i < 3; i++) m.e[j][i] -= d * m.e[r][i];
+        }
+    }
+    cd d = det3(m);
+    double t = std::arg(d) / 3.0;
+    cd ph(std::cos(-t), std::sin(-t));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m.e[i][j] *= ph;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------ generators
+
+// Links U_mu(x) = reunitarize(exp(eps * A)), A = algebra_expand(xi) with
+// xi_a ~ N(0, 2) (Algebra::gaussian_random default width sqrt(2),
+// sun_matrix.h:548-551), i.e. U = exp(i eps H) with H Hermitian traceless,
+// E|H_ij|^2 = 1 off the diagonal.  Draw order: dir-major, then lexicographic site.
+void or_gen_links(const int *dims, double eps, uint64_t seed, double *U) {
+    Geom g(dims, 0);
+    HostRng rng(seed);
+    std::vector<double> coef((size_t)4 * g.V * 8);
+    const double width = std::sqrt(2.0);
+    for (size_t n = 0; n < coef.size(); n += 2) {
+        double gr;
+        coef[n] = rng.gaussrand2(gr) * width;
+        coef[n + 1] = gr * width;
+    }
+    long nl = 4 * g.V;
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nl; l++) {
+        Mat3 A = algebra_expand(&coef[8 * l]);
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) A.e[i][j] *= eps;
+        Mat3 m = mexp(A);
+        reunitarize(m);
+        double *p = U + 18 * l;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                p[(i * 3 + j) * 2] = m.e[i][j].real();
+                p[(i * 3 + j) * 2 + 1] = m.e[i][j].imag();
+            }
+    }
+}
+
+// Unit gauge U = 1 (test_CG.cpp:62-65).
+void or_unit_links(const int *dims, double *U) {
+    Geom g(dims, 0);
+    std::memset(U, 0, sizeof(double) * 18 * 4 * g.V);
+    for (long l = 0; l < 4 * g.V; l++)
+        for (int i = 0; i < 3; i++) U[18 * l + (i * 3 + i) * 2] = 1.0;
+}
+
+// Gaussian spinor: every complex entry from Complex::gaussian_random
+// (re = r sin phi, im = r cos phi; cmplx.h:344-349), spin-major then colour,
+// sites in lexicographic order; sites outside parity_mask are zero.
+void or_gen_spinor(const int *dims, uint64_t seed, int parity_mask, double *psi) {
+    Geom g(dims, 0);
+    HostRng rng(seed);
+    for (long i = 0; i < g.V; i++) {
+        double *p = psi + 24 * i;
+        if (!g.in(i, parity_mask)) {
+            std::memset(p, 0, 24 * sizeof(double));
+            continue;
+        }
+        for (int c = 0; c < 12; c++) {
+            double d;
+            p[2 * c] = rng.gaussrand2(d);
+            p[2 * c + 1] = d;
+        }
+    }
+}
+
+// ------------------------------------------------------------ site algebra
+
+// gamma g (0..3 = gamma0..gamma3, 4 = gamma5) acting on one spinor, wilson_vector.h:311-347
+void or_gamma(int gm, const double *w_in, double *w_out) {
+    Spinor w = load_spinor(w_in, 0), r;
+    for (int k = 0; k < 3; k++) {
+        switch (gm) {
+        case 0:
+            r.s[0][k] = w.s[2][k];
+            r.s[1][k] = w.s[3][k];
+            r.s[2][k] = w.s[0][k];
+            r.s[3][k] = w.s[1][k];
+            break;
+        case 1:
+            r.s[0][k] = I1 * w.s[3][k];
+            r.s[1][k] = I1 * w.s[2][k];
+            r.s[2][k] = -I1 * w.s[1][k];
+            r.s[3][k] = -I1 * w.s[0][k];
+            break;
+        case 2:
+            r.s[0][k] = -w.s[3][k];
+            r.s[1][k] = w.s[2][k];
+            r.s[2][k] = w.s[1][k];
+            r.s[3][k] = -w.s[0][k];
+            break;
+        case 3:
+            r.s[0][k] = I1 * w.s[2][k];
+            r.s[1][k] = -I1 * w.s[3][k];
+            r.s[2][k] = -I1 * w.s[0][k];
+            r.s[3][k] = I1 * w.s[1][k];
+            break;
+        default:
+            r.s[0][k] = w.s[0][k];
+            r.s[1][k] = w.s[1][k];
+            r.s[2][k] = -w.s[2][k];
+            r.s[3][k] = -w.s[3][k];
+            break;
+        }
+    }
+    store_spinor(w_out, 0, r);
+}
+
+// half-spinor projection (12 doubles out) and expansion (24 doubles out);
+// dir 0..3 = x,y,z,t
+void or_project(const double *w_in, int dir, int sign, double *h_out) {
+    Half h = project(load_spinor(w_in, 0), dir, sign);
+    for (int a = 0; a < 2; a++)
+        for (int k = 0; k < 3; k++) {
+            h_out[(a * 3 + k) * 2] = h.c[a][k].real();
+            h_out[(a * 3 + k) * 2 + 1] = h.c[a][k].imag();
+        }
+}
+void or_expand(const double *h_in, int dir, int sign, double *w_out) {
+    Half h;
+    for (int a = 0; a < 2; a++)
+        for (int k = 0; k < 3; k++) h.c[a][k] = cd(h_in[(a * 3 + k) * 2], h_in[(a * 3 + k) * 2 + 1]);
+    store_spinor(w_out, 0, expand(h, dir, sign));
+}
+// colour matrix times each colour vector of a half spinor
+void or_mul_half(const double *U_in, const double *h_in, double *h_out) {
+    Mat3 U = load_link(U_in, 1, 0, 0);
+    Half h;
+    for (int a = 0; a < 2; a++)
+        for (int k = 0; k < 3; k++) h.c[a][k] = cd(h_in[(a * 3 + k) * 2], h_in[(a * 3 + k) * 2 + 1]);
+    Half r = mul(U, h);
+    for (int a = 0; a < 2; a++)
+        for (int k = 0; k < 3; k++) {
+            h_out[(a * 3 + k) * 2] = r.c[a][k].real();
+            h_out[(a * 3 + k) * 2 + 1] = r.c[a][k].imag();
+        }
+}
+
+// ------------------------------------------------------------ operators
+
+// Dirac_Wilson_hop (set=0: out[par] -= kappa H_s in) and
+// Dirac_Wilson_hop_set (set=1: out[par] = -kappa H_s in), wilson.h:15-95.
+void or_wilson_hop(const int *dims, int tap, const double *U, double kappa, const double *in,
+                   double *out, int par, int sign, int set) {
+    Geom g(dims, tap);
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        if (!g.in(x, par)) continue;
+        Spinor h = hop_site(g, U, in, x, sign);
+        Spinor o;
+        if (set) {
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 3; b++) o.s[a][b] = -kappa * h.s[a][b];
+        } else {
+            o = load_spinor(out, x);
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 3; b++) o.s[a][b] -= kappa * h.s[a][b];
+        }
+        store_spinor(out, x, o);
+    }
+}
+
+// Dirac_Wilson::apply / dagger (sign=+1 / -1): D_s = 1 - kappa H_s over ALL, wilson.h:183-192
+void or_wilson_apply(const int *dims, int tap, const double *U, double kappa, const double *in,
+                     double *out, int sign) {
+    Geom g(dims, tap);
+    std::memcpy(out, in, sizeof(double) * 24 * g.V);
+    or_wilson_hop(dims, tap, U, kappa, in, out, 3, sign, 0);
+}
+
+// Dirac_Wilson_evenodd::apply / dagger, wilson.h:272-289.  in, out are full
+// lattice fields; out[EVEN] = in_e - kappa^2 H^{eo}_s H^{oe}_s in_e, out[ODD] = 0.
+void or_wilson_eo_apply(const int *dims, int tap, const double *U, double kappa,
+                        const double *in, double *out, int sign) {
+    Geom g(dims, tap);
+    std::vector<double> tmp((size_t)24 * g.V, 0.0);
+    // Dirac_Wilson_diag(in, out, EVEN)
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 1)) std::memcpy(out + 24 * x, in + 24 * x, 24 * sizeof(double));
+    // hop_set(kappa, in, tmp, ODD, s); diag_inverse is a no-op
+    or_wilson_hop(dims, tap, U, kappa, in, tmp.data(), 2, sign, 1);
+    // hop(-kappa, tmp, out, EVEN, s)
+    or_wilson_hop(dims, tap, U, -kappa, tmp.data(), out, 1, sign, 0);
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 2)) std::memset(out + 24 * x, 0, 24 * sizeof(double));
+}
+
+// sum over sites of parity par of conj(a) . b  (WilsonVector::dot, conj-linear in a)
+void or_dot(const int *dims, const double *a, const double *b, int par, double *re, double *im) {
+    Geom g(dims, 0);
+    double sr = 0, si = 0;
+#pragma omp parallel for reduction(+ : sr, si) schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        if (!g.in(x, par)) continue;
+        for (int c = 0; c < 12; c++) {
+            double ar = a[24 * x + 2 * c], ai = a[24 * x + 2 * c + 1];
+            double br = b[24 * x + 2 * c], bi = b[24 * x + 2 * c + 1];
+            sr += ar * br + ai * bi;
+            si += ar * bi - ai * br;
+        }
+    }
+    *re = sr;
+    *im = si;
+}
+
+double or_squarenorm(const int *dims, const double *a, int par) {
+    double re, im;
+    or_dot(dims, a, a, par, &re, &im);
+    return re;
+}
+
+// CG<Dirac_Wilson_evenodd>::apply(in, out), conjugate_gradient.h:46-104:
+// solves M^dagger M out = in on EVEN sites, out is the initial guess on entry.
+// Stops when |r|^2 < acc^2 |in|^2 or after maxiters iterations.  Returns the
+// iteration count; *rr_out = final |r|^2 / |in|^2 (the quantity the reference
+// prints as "relative residue", conjugate_gradient.h:103).
+int or_cg(const int *dims, int tap, const double *U, double kappa, const double *in, double *out,
+          double acc, int maxiters, double *rr_out) {
+    Geom g(dims, tap);
+    size_t n = (size_t)24 * g.V;
+    std::vector<double> r(n, 0.0), p(n, 0.0), Dp(n, 0.0), DDp(n, 0.0);
+    double source_norm = or_squarenorm(dims, in, 1);
+    double target_rr = acc * acc * source_norm;
+    or_wilson_eo_apply(dims, tap, U, kappa, out, Dp.data(), 1);
+    or_wilson_eo_apply(dims, tap, U, kappa, Dp.data(), DDp.data(), -1);
+    for (long x = 0; x < g.V; x++) {
+        if (!g.in(x, 1)) continue;
+        for (int c = 0; c < 24; c++) {
+            r[24 * x + c] = in[24 * x + c] - DDp[24 * x + c];
+            p[24 * x + c] = r[24 * x + c];
+        }
+    }
+    double rr = or_squarenorm(dims, r.data(), 1), rrnew = rr;
+    int i;
+    for (i = 0; i < maxiters; i++) {
+        or_wilson_eo_apply(dims, tap, U, kappa, p.data(), Dp.data(), 1);
+        or_wilson_eo_apply(dims, tap, U, kappa, Dp.data(), DDp.data(), -1);
+        double pDp = or_squarenorm(dims, Dp.data(), 1);
+        double alpha = rr / pDp;
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, 1)) continue;
+            for (int c = 0; c < 24; c++) {
+                out[24 * x + c] += alpha * p[24 * x + c];
+                r[24 * x + c] -= alpha * DDp[24 * x + c];
+            }
+        }
+        rrnew = or_squarenorm(dims, r.data(), 1);
+        if (rrnew < target_rr) break;
+        double beta = rrnew / rr;
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, 1)) continue;
+            for (int c = 0; c < 24; c++) p[24 * x + c] = beta * p[24 * x + c] + r[24 * x + c];
+        }
+        rr = rrnew;
+    }
+    if (rr_out) *rr_out = rrnew / source_norm;
+    return i;
+}
+
+// true residual of the even-odd system M_s x = b on EVEN: |b - M_s x| / |b|
+double or_true_residual(const int *dims, int tap, const double *U, double kappa, const double *b,
+                        const double *x, int sign) {
+    Geom g(dims, tap);
+    std::vector<double> Mx((size_t)24 * g.V);
+    or_wilson_eo_apply(dims, tap, U, kappa, x, Mx.data(), sign);
+    double num = 0, den = 0;
+    for (long s = 0; s < g.V; s++) {
+        if (!g.in(s, 1)) continue;
+        for (int c = 0; c < 24; c++) {
+            double d = b[24 * s + c] - Mx[24 * s + c];
+            num += d * d;
+            den += b[24 * s + c] * b[24 * s + c];
+        }
+    }
+    return std::sqrt(num / den);
+}
+
+// true residual of the normal system M^dagger M x = b on EVEN
+double or_true_residual_normal(const int *dims, int tap, const double *U, double kappa,
+                               const double *b, const double *x) {
+    Geom g(dims, tap);
+    std::vector<double> t((size_t)24 * g.V), AX((size_t)24 * g.V);
+    or_wilson_eo_apply(dims, tap, U, kappa, x, t.data(), 1);
+    or_wilson_eo_apply(dims, tap, U, kappa, t.data(), AX.data(), -1);
+    double num = 0, den = 0;
+    for (long s = 0; s < g.V; s++) {
+        if (!g.in(s, 1)) continue;
+        for (int c = 0; c < 24; c++) {
+            double d = b[24 * s + c] - AX[24 * s + c];
+            num += d * d;
+            den += b[24 * s + c] * b[24 * s + c];
+        }
+    }
+    return std::sqrt(num / den);
+}
+
+// ------------------------------------------------------------ reference-structured variant
+//
+// Same operator, organised the way the reference's generated loops run it
+// (wilson.h:53-95 + conjugate_gradient.h): eight temporary half-spinor fields,
+// for every direction one projection loop and one U^dagger-projection loop over
+// the source parity, neighbour-index gathers from precomputed neighbour arrays
+// (lattice.cpp:971-992) with the antiperiodic values negated by a separate
+// gather pass (field_storage_backend.h gather_elements_negated), then one
+// accumulate loop per direction over the target parity.  Used only as the
+// timed CPU baseline; its results equal or_wilson_eo_apply's.
+
+struct RefWorkspace {
+    Geom g;
+    std::vector<long> nbr[8];       // neighbour index arrays, dir and opp dir
+    std::vector<double> nsign[8];   // boundary sign per site and direction
+    std::vector<double> vtemp[8];   // 8 half-spinor fields, 12 doubles per site
+    std::vector<double> tmp;
+    RefWorkspace(const int *dims, int tap) : g(dims, tap) {
+        for (int d = 0; d < 8; d++) {
+            nbr[d].resize(g.V);
+            nsign[d].resize(g.V);
+            vtemp[d].resize((size_t)12 * g.V);
+        }
+        for (long x = 0; x < g.V; x++)
+            for (int mu = 0; mu < 4; mu++) {
+                double s;
+                nbr[mu][x] = g.nb(x, mu, +1, &s);
+                nsign[mu][x] = s;
+                nbr[7 - mu][x] = g.nb(x, mu, -1, &s);
+                nsign[7 - mu][x] = s;
+            }
+        tmp.resize((size_t)24 * g.V);
+    }
+};
+
+static void ref_hop(RefWorkspace &w, const double *U, double kappa, const double *in, double *out,
+                    int par, int sign, int set) {
+    const Geom &g = w.g;
+    const int opp = par == 1 ? 2 : 1;
+    for (int mu = 0; mu < 4; mu++) {
+        // onsites(opp_parity(par)) vtemp[-dir][X] = U_dir(X)^dagger * proj(in, dir, -sign)
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, opp)) continue;
+            Half h = mul_adj(load_link(U, g.V, mu, x), project(load_spinor(in, x), mu, -sign));
+            double *p = &w.vtemp[7 - mu][12 * x];
+            for (int a = 0; a < 2; a++)
+                for (int k = 0; k < 3; k++) {
+                    p[(a * 3 + k) * 2] = h.c[a][k].real();
+                    p[(a * 3 + k) * 2 + 1] = h.c[a][k].imag();
+                }
+        }
+        // onsites(opp_parity(par)) vtemp[dir][X] = proj(in, dir, sign)
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, opp)) continue;
+            Half h = project(load_spinor(in, x), mu, sign);
+            double *p = &w.vtemp[mu][12 * x];
+            for (int a = 0; a < 2; a++)
+                for (int k = 0; k < 3; k++) {
+                    p[(a * 3 + k) * 2] = h.c[a][k].real();
+                    p[(a * 3 + k) * 2 + 1] = h.c[a][k].imag();
+                }
+        }
+    }
+    for (int mu = 0; mu < 4; mu++) {
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, par)) continue;
+            long yf = w.nbr[mu][x], yb = w.nbr[7 - mu][x];
+            double sf = w.nsign[mu][x], sb = w.nsign[7 - mu][x];
+            Half hf, hb;
+            for (int a = 0; a < 2; a++)
+                for (int k = 0; k < 3; k++) {
+                    hf.c[a][k] = sf * cd(w.vtemp[mu][12 * yf + (a * 3 + k) * 2],
+                                         w.vtemp[mu][12 * yf + (a * 3 + k) * 2 + 1]);
+                    hb.c[a][k] = sb * cd(w.vtemp[7 - mu][12 * yb + (a * 3 + k) * 2],
+                                         w.vtemp[7 - mu][12 * yb + (a * 3 + k) * 2 + 1]);
+                }
+            Spinor ef = expand(mul(load_link(U, g.V, mu, x), hf), mu, sign);
+            Spinor eb = expand(hb, mu, -sign);
+            Spinor o = load_spinor(out, x);
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 3; b++) {
+                    cd v = kappa * (ef.s[a][b] + eb.s[a][b]);
+                    o.s[a][b] = (set && mu == 0) ? -v : o.s[a][b] - v;
+                }
+            store_spinor(out, x, o);
+        }
+    }
+}
+
+void *or_ref_create(const int *dims, int tap) { return new RefWorkspace(dims, tap); }
+void or_ref_destroy(void *ws) { delete (RefWorkspace *)ws; }
+
+// Dirac_Wilson_evenodd::apply / dagger in the reference's loop structure
+void or_ref_eo_apply(void *ws, const double *U, double kappa, const double *in, double *out,
+                     int sign) {
+    RefWorkspace &w = *(RefWorkspace *)ws;
+    const Geom &g = w.g;
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 1)) std::memcpy(out + 24 * x, in + 24 * x, 24 * sizeof(double));
+    ref_hop(w, U, kappa, in, w.tmp.data(), 2, sign, 1);
+    ref_hop(w, U, -kappa, w.tmp.data(), out, 1, sign, 0);
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 2)) std::memset(out + 24 * x, 0, 24 * sizeof(double));
+}
+
+// Reference-structured CG: or_cg's algorithm with the reference-structured
+// operator.  Runs at most maxiters iterations; returns the count.
+int or_ref_cg(void *ws, const double *U, double kappa, const double *in, double *out, double acc,
+              int maxiters, double *rr_out) {
+    RefWorkspace &w = *(RefWorkspace *)ws;
+    const Geom &g = w.g;
+    int dims[4] = {g.L[0], g.L[1], g.L[2], g.L[3]};
+    size_t n = (size_t)24 * g.V;
+    std::vector<double> r(n, 0.0), p(n, 0.0), Dp(n, 0.0), DDp(n, 0.0);
+    double source_norm = or_squarenorm(dims, in, 1);
+    double target_rr = acc * acc * source_norm;
+    or_ref_eo_apply(ws, U, kappa, out, Dp.data(), 1);
+    or_ref_eo_apply(ws, U, kappa, Dp.data(), DDp.data(), -1);
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        if (!g.in(x, 1)) continue;
+        for (int c = 0; c < 24; c++) {
+            r[24 * x + c] = in[24 * x + c] - DDp[24 * x + c];
+            p[24 * x + c] = r[24 * x + c];
+        }
+    }
+    double rr = or_squarenorm(dims, r.data(), 1), rrnew = rr;
+    int i;
+    for (i = 0; i < maxiters; i++) {
+        or_ref_eo_apply(ws, U, kappa, p.data(), Dp.data(), 1);
+        or_ref_eo_apply(ws, U, kappa, Dp.data(), DDp.data(), -1);
+        double pDp = or_squarenorm(dims, Dp.data(), 1);
+        double alpha = rr / pDp;
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, 1)) continue;
+            for (int c = 0; c < 24; c++) {
+                out[24 * x + c] += alpha * p[24 * x + c];
+                r[24 * x + c] -= alpha * DDp[24 * x + c];
+            }
+        }
+        rrnew = or_squarenorm(dims, r.data(), 1);
+        if (rrnew < target_rr) break;
+        double beta = rrnew / rr;
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < g.V; x++) {
+            if (!g.in(x, 1)) continue;
+            for (int c = 0; c < 24; c++) p[24 * x + c] = beta * p[24 * x + c] + r[24 * x + c];
+        }
+        rr = rrnew;
+    }
+    if (rr_out) *rr_out = rrnew / source_norm;
+    return i;
+}
+
+int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void or_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+}  // extern "C"
