@@ -10,6 +10,9 @@ benchmark configurations; no external data):
           metric: CG solves/s.
   dslash  32^4, the even-odd operator applied with its dagger; one step =
           100 x (apply + dagger).  metric: dslash HBM GB/s (algorithmic bytes).
+  mrhs    the cg workload with 12 Gaussian sources per step solved together by the
+          batched mixed-precision engine (FP16 inner solve by default).
+          metric: CG solves/s.
   cg8     8^4, kappa = 0.12, plain FP64 CG (the CPU-runnable configuration).
 
 Multi-GPU runs (torchrun) are replicas: every rank solves its own copy of the
@@ -38,13 +41,14 @@ METRIC = "CG solves/s at 1e-10 residual (mixed vs FP64), dslash HBM GB/s, p50/p9
 
 WORKLOADS = {
     "cg": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101),
+    "mrhs": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101, nrhs=12),
     "cg8": dict(dims=(8, 8, 8, 8), eps=0.3, kappa=0.12, tol=1e-10, link_seed=1, src_seed=2),
     "dslash": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=None, link_seed=100, src_seed=101),
 }
 # CG iterations of one solve of each workload (FP64 CG on M^dag M, true residual 1e-10), used to turn the
 # reference arm's per-iteration time into solves/s.  Measured by the FP64 GPU CG on exactly these seeded
 # inputs; the CPU runs the same algorithm, so the count is the same.
-ITERS_PER_SOLVE = {"cg": None, "cg8": None}
+ITERS_PER_SOLVE = {"cg": 59, "mrhs": 59, "cg8": None}
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -248,10 +252,69 @@ def run_ours(args, dist: Dist):
         e2e = None
         dtype = "f64"
         roof_ms = ms_apply
+    elif args.workload == "mrhs":
+        nrhs = w["nrhs"]
+        srcs = [b_host] + [hw.generate_spinor(dims, w["src_seed"] + k, hw.EVEN) for k in range(1, nrhs)]
+        fbs = [hw.Field(lat, s_) for s_ in srcs]
+        fxs = [hw.Field(lat) for _ in range(nrhs)]
+        prec = args.precision if args.precision != "f64" else "f16"
+
+        def batch_once():
+            for f in fxs:
+                f.zero()
+            return hw.batch_solve(ctx, [(D, fbs[k], fxs[k], w["tol"]) for k in range(nrhs)], precision=prec)
+
+        for _ in range(args.warmup):
+            batch_once()
+        dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        res = []
+        for _ in range(args.steps):
+            res += batch_once()
+        ev1.record(stream)
+        ev1.synchronize()
+        clk = clocks.stop()
+        t = dist.max(ev0.elapsed_time(ev1) * 1e-3)
+        value = dist.world * args.steps * nrhs / t
+        ms_per_step = t / args.steps * 1e3
+        unit = "solves/s"
+        launches = sum(r.kernel_launches for r in res) // nrhs
+        lat_ms = sorted(1e3 * r.seconds for r in res)
+        result.update(iterations=max(r.iterations for r in res), reliable_updates=max(r.reliable_updates for r in res),
+                      true_residual=max(r.true_residual for r in res), all_converged=all(r.converged for r in res),
+                      precision=prec, nrhs=nrhs, latency_ms_p50=lat_ms[len(lat_ms) // 2],
+                      latency_ms_p99=lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))])
+        dtype = {"f32": "f32+f64", "f16": "f16+f64"}[prec]
+        # e2e: host sources in, host solutions out, through the public API
+        pins = [hw.PinnedArray((V, 4, 3, 2)) for _ in range(nrhs)]
+        pouts = [hw.PinnedArray((V, 4, 3, 2)) for _ in range(nrhs)]
+        for k in range(nrhs):
+            pins[k].array[:] = srcs[k]
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for k in range(nrhs):
+                fbs[k].upload(pins[k].array, hw.EVEN)
+            batch_once()
+            for k in range(nrhs):
+                fxs[k].download(hw.ALL, pouts[k].array)
+        t_e2e = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.world * args.steps * nrhs / t_e2e, "unit": "solves/s",
+               "h2d_bytes_per_step": int(nrhs * pins[0].array.nbytes),
+               "d2h_bytes_per_step": int(nrhs * pouts[0].array.nbytes)}
+        for pa in pins + pouts:
+            pa.free()
+        roof_ms = dslash_time(50)
+        result["dslash_ms_per_apply"] = roof_ms
+        for f in fbs + fxs:
+            f.close()
     else:
         def solve_once():
             fx.zero()
-            return D.solve(fb, fx, accuracy=w["tol"], precision=args.precision)
+            return D.solve(fb, fx, accuracy=w["tol"], precision=args.precision, use_graph=not args.no_graph)
 
         for _ in range(args.warmup):
             r = solve_once()
@@ -376,6 +439,7 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
     ap.add_argument("--link-format", type=int, default=18, choices=[18, 12])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="FP64 CG iterations from a host loop (for launch lists)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

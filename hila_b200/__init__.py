@@ -72,6 +72,11 @@ class _CgResult(ctypes.Structure):
                 ("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_int)]
 
 
+class _SolveRequest(ctypes.Structure):
+    _fields_ = [("gauge", ctypes.c_void_p), ("kappa", ctypes.c_double), ("b", ctypes.c_void_p),
+                ("x", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int)]
+
+
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -106,6 +111,8 @@ _SIGNATURES = {
                                                ctypes.POINTER(_CgResult)]),
     "hw_wilson_evenodd_solve_host": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp, ctypes.POINTER(_CgParams),
                                                     ctypes.POINTER(_CgResult)]),
+    "hw_batch_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_SolveRequest),
+                                      ctypes.c_int, ctypes.POINTER(_CgResult)]),
     "hw_generate_links": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_uint64, _dp]),
     "hw_generate_spinor": (ctypes.c_int, [_ip, ctypes.c_uint64, ctypes.c_int, _dp]),
 }
@@ -439,3 +446,23 @@ class CG:
             _check(rc)
         self.last = CGResult.from_c(r)
         return self.last
+
+
+def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0.1) -> list:
+    """Solve many M x = b at once: requests are (op, b_field, x_field[, accuracy[, maxiters]]).
+
+    All right-hand sides on all lattices advance together, one kernel launch
+    per CG phase (hw_batch_solve); returns one CGResult per request.
+    """
+    n = len(requests)
+    arr = (_SolveRequest * max(n, 1))()
+    for k, req in enumerate(requests):
+        op, b, x = req[0], req[1], req[2]
+        acc = req[3] if len(req) > 3 else 1e-10
+        mi = req[4] if len(req) > 4 else 10000
+        arr[k] = _SolveRequest(op.gauge.handle.value, op.kappa, b.handle.value, x.handle.value, float(acc), int(mi))
+    res = (_CgResult * max(n, 1))()
+    rc = lib().hw_batch_solve(ctx.handle, PRECISIONS[precision], float(delta), arr, n, res)
+    if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+        _check(rc)
+    return [CGResult.from_c(res[k]) for k in range(n)]

@@ -1,6 +1,7 @@
 // C-ABI entry points: contexts, lattices, fields and the FP64 operators.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 
 #include "hw_internal.h"
@@ -50,6 +51,41 @@ int ensure_workspace(hw_lattice *lat) {
     for (HalfBuf *h : {&w.r, &w.p, &w.Dp, &w.DDp, &w.src, &w.res, &w.t})
         if ((rc = alloc_half(*h, lat->stride)) != HW_OK) return rc;
     w.allocated = true;
+    return HW_OK;
+}
+
+int tune_hop(hw_lattice *lat, const hw_gauge *G) {
+    if (lat->tuned) return HW_OK;
+    lat->tuned = true;
+    if (const char *env = std::getenv("HW_HOP_VARIANT")) {
+        int v = std::atoi(env);
+        lat->g.hop_variant = (v >= 0 && v < kHopVariants) ? v : 0;
+        return HW_OK;
+    }
+    int rc;
+    if ((rc = ensure_workspace(lat)) != HW_OK) return rc;
+    hw_context *ctx = lat->ctx;
+    CgWorkspace &w = *lat->ws;
+    HW_CUDA(cudaMemsetAsync(w.p.buf.ptr, 0, w.p.buf.bytes, ctx->stream));
+    float best = 1e30f;
+    int best_v = 0;
+    for (int v = 0; v < kHopVariants; v++) {
+        Geom g = lat->g;
+        g.hop_variant = v;
+        for (int k = 0; k < 2; k++) launch_hop_scale(g, G->U(), 1, +1, w.p.h(), w.t.h(), 1.0, nullptr, ctx->stream);
+        HW_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int k = 0; k < 5; k++) launch_hop_scale(g, G->U(), 1, +1, w.p.h(), w.t.h(), 1.0, nullptr, ctx->stream);
+        HW_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+        HW_CUDA(cudaEventSynchronize(ctx->ev1));
+        float ms = 0;
+        HW_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    HW_CUDA(cudaGetLastError());
+    lat->g.hop_variant = best_v;
     return HW_OK;
 }
 
@@ -123,6 +159,7 @@ int hw_context_destroy(hw_context *ctx) {
     if (!ctx) return HW_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    destroy_engines(ctx);
     if (ctx->cg_state_host) cudaFreeHost(ctx->cg_state_host);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -321,6 +358,7 @@ static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_fiel
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     HW_CUDA(cudaSetDevice(ctx->device));
     if ((rc = ensure_workspace(lat)) != HW_OK) return rc;
+    if ((rc = tune_hop(lat, G)) != HW_OK) return rc;
     CgWorkspace &w = *lat->ws;
     // t_o = H^{oe}_s in_e ; out_e = in_e - kappa^2 H^{eo}_s t_o ; out_o = 0  (wilson.h:272-279)
     launch_hop_scale(lat->g, G->U(), 1, sign, in->half[0].h(), w.t.h(), 1.0, nullptr, ctx->stream);
@@ -349,6 +387,7 @@ int hw_wilson_apply(const hw_gauge *G, double kappa, int sign, const hw_field *i
     hw_context *ctx = lat->ctx;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     HW_CUDA(cudaSetDevice(ctx->device));
+    if ((rc = tune_hop(lat, G)) != HW_OK) return rc;
     // out_p = in_p - kappa H_s in_{1-p} for both parities (wilson.h:183-192)
     for (int p = 0; p < 2; p++)
         launch_hop_xpay(lat->g, G->U(), p, sign, in->half[1 - p].h(), in->half[p].h(), out->half[p].h(), -kappa,

@@ -34,6 +34,15 @@ struct EpiScale {
     __device__ void operator()(const double *) {}
 };
 
+// Component c (0..11) of a half-lattice FP64 field at site i
+__device__ __forceinline__ Cx<double> load_c(const SpinorF64 &f, int c, int i) {
+    double2 v = f.p[(size_t)c * f.stride + i];
+    return {v.x, v.y};
+}
+__device__ __forceinline__ void store_c(const SpinorF64 &f, int c, int i, Cx<double> v) {
+    f.p[(size_t)c * f.stride + i] = make_double2(v.re, v.im);
+}
+
 // out = x + b * H in ; optionally pAp = |out|^2 and alpha = rr / pAp
 template <bool RED>
 struct EpiXpay {
@@ -43,16 +52,13 @@ struct EpiXpay {
     CgState *st;
     __device__ bool skip() const { return st && st->status != CG_RUNNING; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
-        Spinor<double> w;
-        x.load_cached(i, w);
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> v = w.s[c / 3][c % 3] + b * acc.s[c / 3][c % 3];
-            acc.s[c / 3][c % 3] = v;
+            Cx<double> v = load_c(x, c, i) + b * acc.s[c / 3][c % 3];
+            store_c(out, c, i, v);
             n2 += norm2(v);
         }
-        out.store(i, acc);
         if (RED) red[0] = n2;
     }
     __device__ void operator()(const double *tot) {
@@ -76,23 +82,15 @@ struct EpiCgUpdate {
     __device__ bool skip() const { return st->status != CG_RUNNING; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
         const double alpha = st->alpha;
-        Spinor<double> w;
-        Dp.load_cached(i, w);
         double n2 = 0;
-        Spinor<double> rr, xx, pp;
-        r.load_cached(i, rr);
-        x.load_cached(i, xx);
-        p.load_cached(i, pp);
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            const int s = c / 3, k = c % 3;
-            Cx<double> ddp = w.s[s][k] + b * acc.s[s][k];
-            rr.s[s][k] = rr.s[s][k] - alpha * ddp;
-            xx.s[s][k] = xx.s[s][k] + alpha * pp.s[s][k];
-            n2 += norm2(rr.s[s][k]);
+            Cx<double> ddp = load_c(Dp, c, i) + b * acc.s[c / 3][c % 3];
+            Cx<double> rv = load_c(r, c, i) - alpha * ddp;
+            store_c(r, c, i, rv);
+            store_c(x, c, i, load_c(x, c, i) + alpha * load_c(p, c, i));
+            n2 += norm2(rv);
         }
-        r.store(i, rr);
-        x.store(i, xx);
         red[0] = n2;
     }
     __device__ void operator()(const double *tot) {
@@ -120,19 +118,15 @@ struct EpiResidual {
     CgState *st;
     __device__ bool skip() const { return false; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
-        Spinor<double> w, sv;
-        x.load_cached(i, w);
-        src.load_cached(i, sv);
         double n2 = 0, d2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            const int s = c / 3, k = c % 3;
-            Cx<double> v = sv.s[s][k] - (w.s[s][k] + b * acc.s[s][k]);
-            acc.s[s][k] = v;
+            Cx<double> sv = load_c(src, c, i);
+            Cx<double> v = sv - (load_c(x, c, i) + b * acc.s[c / 3][c % 3]);
+            if (res.p) store_c(res, c, i, v);
             n2 += norm2(v);
-            d2 += norm2(sv.s[s][k]);
+            d2 += norm2(sv);
         }
-        if (res.p) res.store(i, acc);
         red[0] = n2;
         red[1] = d2;
     }
@@ -142,10 +136,10 @@ struct EpiResidual {
     }
 };
 
-template <int SIGN, class Lk, class Epi>
-__global__ void __launch_bounds__(kHopBlock) k_hop(Geom g, Lk U, int par, SpinorF64 in, Epi epi, RedBuf red) {
+template <int SIGN, int BLOCK, int MINB, class Lk, class Epi>
+__global__ void __launch_bounds__(BLOCK, MINB) k_hop(Geom g, Lk U, int par, SpinorF64 in, Epi epi, RedBuf red) {
     if (epi.skip()) return;
-    const int i = blockIdx.x * kHopBlock + threadIdx.x;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
     double v[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
     for (int k = 0; k < (Epi::NRED > 0 ? Epi::NRED : 1); k++) v[k] = 0.0;
@@ -154,28 +148,47 @@ __global__ void __launch_bounds__(kHopBlock) k_hop(Geom g, Lk U, int par, Spinor
         hop_site<SIGN>(g, par, i, in, U, acc);
         epi(i, acc, v);
     }
-    if constexpr (Epi::NRED > 0) grid_reduce<Epi::NRED, kHopBlock>(v, red.partials, red.ticket, epi);
+    if constexpr (Epi::NRED > 0) grid_reduce<Epi::NRED, BLOCK>(v, red.partials, red.ticket, epi);
+}
+
+template <int BLOCK, int MINB, class Lk, class Epi>
+void launch_variant(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin, const Epi &epi, RedBuf rb,
+                    cudaStream_t s) {
+    dim3 grid((g.Vh + BLOCK - 1) / BLOCK);
+    if (sign > 0)
+        k_hop<1, BLOCK, MINB><<<grid, BLOCK, 0, s>>>(g, L, par, sin, epi, rb);
+    else
+        k_hop<-1, BLOCK, MINB><<<grid, BLOCK, 0, s>>>(g, L, par, sin, epi, rb);
+}
+
+// Launch shapes the autotuner chooses from (HopVariant in kernels.h):
+//   0: 128 threads, registers unconstrained   1: 128 threads, <= 128 registers (4 blocks/SM)
+//   2: 256 threads, <= 128 registers
+template <class Lk, class Epi>
+void launch_shape(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin, const Epi &epi, RedBuf rb,
+                  cudaStream_t s) {
+    switch (g.hop_variant) {
+    case 1:
+        launch_variant<128, 4>(g, L, par, sign, sin, epi, rb, s);
+        break;
+    case 2:
+        launch_variant<256, 2>(g, L, par, sign, sin, epi, rb, s);
+        break;
+    default:
+        launch_variant<128, 1>(g, L, par, sign, sin, epi, rb, s);
+        break;
+    }
 }
 
 template <class Epi>
 void dispatch_hop(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, const Epi &epi, const RedBuf *red,
                   cudaStream_t s) {
-    dim3 grid((g.Vh + kHopBlock - 1) / kHopBlock);
     RedBuf rb = red ? *red : RedBuf{nullptr, nullptr};
     SpinorF64 sin{in.p, in.stride};
-    if (U.planes == 9) {
-        LinksF64x18 L{U.p, U.stride};
-        if (sign > 0)
-            k_hop<1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
-        else
-            k_hop<-1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
-    } else {
-        LinksF64x12 L{U.p, U.stride};
-        if (sign > 0)
-            k_hop<1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
-        else
-            k_hop<-1><<<grid, kHopBlock, 0, s>>>(g, L, par, sin, epi, rb);
-    }
+    if (U.planes == 9)
+        launch_shape(g, LinksF64x18{U.p, U.stride}, par, sign, sin, epi, rb, s);
+    else
+        launch_shape(g, LinksF64x12{U.p, U.stride}, par, sign, sin, epi, rb, s);
 }
 
 // ------------------------------------------------------------------ vectors

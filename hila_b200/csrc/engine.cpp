@@ -1,0 +1,368 @@
+// Host side of the batched mixed-precision CG engine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine_host.h"
+
+namespace hw {
+
+int ensure_low_links(const hw_gauge *G, int low) {
+    hw_lattice *lat = G->lat;
+    hw_context *ctx = lat->ctx;
+    const size_t st = lat->stride;
+    int rc;
+    if (low == LOW_F32 && !G->f32.ptr) {
+        if ((rc = G->f32.alloc(24 * st * sizeof(float4))) != HW_OK) return rc;
+        eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, G->f32.as<float4>(), nullptr,
+                          nullptr, ctx->stream);
+    }
+    if (low == LOW_F16 && !G->f16a.ptr) {
+        if ((rc = G->f16a.alloc(8 * st * sizeof(uint4))) != HW_OK) return rc;
+        if ((rc = G->f16b.alloc(8 * st * sizeof(uint2))) != HW_OK) return rc;
+        eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, nullptr, G->f16a.as<uint4>(),
+                          G->f16b.as<uint2>(), ctx->stream);
+    }
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+Engine::~Engine() {
+    if (ctx_) {
+        cudaSetDevice(ctx_->device);
+        cudaStreamSynchronize(ctx_->stream);
+    }
+    if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
+    if (pinned_states_) cudaFreeHost(pinned_states_);
+}
+
+int Engine::init() {
+    if (ready_) return HW_OK;
+    int rc;
+    if ((rc = d_tables_.alloc(sizeof(EngTables))) != HW_OK) return rc;
+    if ((rc = d_states_.alloc(sizeof(EngState) * kEngMaxProb)) != HW_OK) return rc;
+    if ((rc = d_tickets_.alloc(sizeof(unsigned) * kEngMaxLat)) != HW_OK) return rc;
+    if ((rc = d_ctl_.alloc(sizeof(int) * 8)) != HW_OK) return rc;
+    HW_CUDA(cudaMemsetAsync(d_tickets_.ptr, 0, d_tickets_.bytes, ctx_->stream));
+    HW_CUDA(cudaMemsetAsync(d_ctl_.ptr, 0, d_ctl_.bytes, ctx_->stream));
+    HW_CUDA(cudaMallocHost(&pinned_states_, sizeof(EngState) * kEngMaxProb));
+    std::memset(&tables_, 0, sizeof(tables_));
+    for (int j = 0; j < kEngMaxProb; j++) {
+        std::memset(&host_states_[j], 0, sizeof(EngState));
+        host_states_[j].status = ENG_IDLE;
+    }
+    HW_CUDA(cudaMemcpyAsync(d_states_.ptr, host_states_, sizeof(host_states_), cudaMemcpyHostToDevice, ctx_->stream));
+    grid_ = eng_grid_size(low_);
+    if ((rc = ensure_partials()) != HW_OK) return rc;
+    ready_ = true;
+    return HW_OK;
+}
+
+int Engine::ensure_partials() {
+    size_t need = std::max<size_t>(tables_.max_tiles, 1);
+    if (d_partials_.ptr && partial_tiles_ >= need) return HW_OK;
+    size_t cap = std::max<size_t>(need, 1024);
+    HW_CUDA(cudaStreamSynchronize(ctx_->stream));
+    int rc = d_partials_.alloc(sizeof(double) * 2 * kEngMaxProb * cap);
+    if (rc != HW_OK) return rc;
+    partial_tiles_ = cap;
+    if (chunk_exec_) {  // pointer changed: rebuild the graph
+        cudaGraphExecDestroy(chunk_exec_);
+        chunk_exec_ = nullptr;
+    }
+    return HW_OK;
+}
+
+int Engine::lattice_index(const hw_gauge *G, int *idx) {
+    for (int l = 0; l < tables_.nlat; l++)
+        if (gauges_[l] == G) {
+            *idx = l;
+            return HW_OK;
+        }
+    HW_CHECK_ARG(tables_.nlat < kEngMaxLat, "engine holds %d lattices already", kEngMaxLat);
+    int rc;
+    if ((rc = ensure_low_links(G, low_)) != HW_OK) return rc;
+    hw_lattice *lat = G->lat;
+    const int l = tables_.nlat;
+    EngLattice &L = tables_.lat[l];
+    std::memset(&L, 0, sizeof(L));
+    L.g = lat->g;
+    L.stride = lat->stride;
+    L.ntiles = (int)((lat->Vh + kEngTile - 1) / kEngTile);
+    L.tile0 = tables_.ntiles;
+    L.nprob = 0;
+    L.l64 = G->f64.as<double2>();
+    L.l64_planes = G->U().planes;
+    L.l32 = G->f32.as<float4>();
+    L.l16a = G->f16a.as<uint4>();
+    L.l16b = G->f16b.as<uint2>();
+    tables_.ntiles += L.ntiles;
+    tables_.max_tiles = std::max(tables_.max_tiles, L.ntiles);
+    tables_.nlat = l + 1;
+    gauges_.push_back(G);
+    tables_dirty_ = true;
+    if ((rc = ensure_partials()) != HW_OK) return rc;
+    *idx = l;
+    return HW_OK;
+}
+
+int Engine::prune_lattices() {
+    // keep lattices that still have used slots; renumber them and their slots
+    std::vector<int> keep;
+    for (int l = 0; l < tables_.nlat; l++) {
+        bool used = false;
+        for (int j = 0; j < kEngMaxProb; j++)
+            if (slots_[j].used && slots_[j].lat == l) used = true;
+        if (used) keep.push_back(l);
+    }
+    if ((int)keep.size() == tables_.nlat) return HW_OK;
+    EngTables nt;
+    std::memset(&nt, 0, sizeof(nt));
+    std::vector<const hw_gauge *> ng;
+    std::vector<int> remap(tables_.nlat, -1);
+    for (int l : keep) {
+        const int k = nt.nlat++;
+        remap[l] = k;
+        nt.lat[k] = tables_.lat[l];
+        nt.lat[k].tile0 = nt.ntiles;
+        nt.ntiles += nt.lat[k].ntiles;
+        nt.max_tiles = std::max(nt.max_tiles, nt.lat[k].ntiles);
+        ng.push_back(gauges_[l]);
+    }
+    std::memcpy(nt.prob, tables_.prob, sizeof(nt.prob));
+    for (int j = 0; j < kEngMaxProb; j++) {
+        if (slots_[j].lat >= 0) slots_[j].lat = remap[slots_[j].lat];
+        if (!slots_[j].used) slots_[j].lat = -1;
+        nt.prob[j].lat = slots_[j].lat;
+    }
+    tables_ = nt;
+    gauges_ = ng;
+    tables_dirty_ = true;
+    return HW_OK;
+}
+
+int Engine::free_slots_on(int lat) const {
+    int used = 0, free_total = 0;
+    for (int j = 0; j < kEngMaxProb; j++) {
+        if (slots_[j].used) {
+            if (slots_[j].lat == lat) used++;
+        } else {
+            free_total++;
+        }
+    }
+    return std::min(kEngMaxRhs - used, free_total);
+}
+
+size_t Engine::slot_bytes(int lat) const {
+    const size_t st = tables_.lat[lat].stride;
+    const size_t low_site = low_ == LOW_F16 ? (48 + 4) : 96;
+    return st * (4 * low_site + 96 + 2 * 192) + st * 2 * 192;  // + owned x, b
+}
+
+int Engine::ensure_slot_buffers(int slot, int stride) {
+    SlotBuffers &B = bufs_[slot];
+    if (B.stride >= stride && B.p.ptr) return HW_OK;
+    const size_t st = stride;
+    int rc;
+    for (DevBuf *d : {&B.x_own, &B.b_own}) d->release();
+    if (low_ == LOW_F16) {
+        for (DevBuf *d : {&B.p, &B.r, &B.Dp, &B.t})
+            if ((rc = d->alloc(3 * st * sizeof(uint4))) != HW_OK) return rc;
+        for (DevBuf *d : {&B.pn, &B.rn, &B.Dpn, &B.tn})
+            if ((rc = d->alloc(st * sizeof(float))) != HW_OK) return rc;
+    } else {
+        for (DevBuf *d : {&B.p, &B.r, &B.Dp, &B.t})
+            if ((rc = d->alloc(6 * st * sizeof(float4))) != HW_OK) return rc;
+        for (DevBuf *d : {&B.pn, &B.rn, &B.Dpn, &B.tn}) d->release();
+    }
+    if ((rc = B.y.alloc(6 * st * sizeof(float4))) != HW_OK) return rc;
+    if ((rc = B.s.alloc(12 * st * sizeof(double2))) != HW_OK) return rc;
+    if ((rc = B.t64.alloc(12 * st * sizeof(double2))) != HW_OK) return rc;
+    B.stride = stride;
+    return HW_OK;
+}
+
+int Engine::ensure_own(int slot) {
+    SlotBuffers &B = bufs_[slot];
+    const size_t bytes = 12 * (size_t)B.stride * sizeof(double2);
+    int rc;
+    if (!B.x_own.ptr || B.x_own.bytes < bytes)
+        if ((rc = B.x_own.alloc(bytes)) != HW_OK) return rc;
+    if (!B.b_own.ptr || B.b_own.bytes < bytes)
+        if ((rc = B.b_own.alloc(bytes)) != HW_OK) return rc;
+    return HW_OK;
+}
+
+int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int maxiter, double delta, int mode,
+                  int *slot_out) {
+    HW_CHECK_ARG(lat >= 0 && lat < tables_.nlat, "bad lattice index");
+    EngLattice &L = tables_.lat[lat];
+    HW_CHECK_ARG(L.nprob < kEngMaxRhs, "lattice holds %d solves already", kEngMaxRhs);
+    int slot = -1;
+    for (int j = 0; j < kEngMaxProb; j++)
+        if (!slots_[j].used) {
+            slot = j;
+            break;
+        }
+    HW_CHECK_ARG(slot >= 0, "no free solve slot (%d in use)", kEngMaxProb);
+    int rc;
+    if ((rc = ensure_slot_buffers(slot, L.stride)) != HW_OK) return rc;
+    SlotBuffers &B = bufs_[slot];
+    if (!b || !x) {
+        if ((rc = ensure_own(slot)) != HW_OK) return rc;
+        if (!b) b = B.b_own.as<double2>();
+        if (!x) x = B.x_own.as<double2>();
+    }
+    EngProblem &P = tables_.prob[slot];
+    std::memset(&P, 0, sizeof(P));
+    P.lat = lat;
+    P.mode = mode;
+    P.kappa = kappa;
+    P.p = B.p.ptr;
+    P.r = B.r.ptr;
+    P.Dp = B.Dp.ptr;
+    P.t = B.t.ptr;
+    P.pn = B.pn.as<float>();
+    P.rn = B.rn.as<float>();
+    P.Dpn = B.Dpn.as<float>();
+    P.tn = B.tn.as<float>();
+    P.y = B.y.as<float4>();
+    P.x = x;
+    P.b = b;
+    P.s = B.s.as<double2>();
+    P.t64 = B.t64.as<double2>();
+    L.prob[L.nprob++] = slot;
+    slots_[slot].used = true;
+    slots_[slot].lat = lat;
+    tables_dirty_ = true;
+
+    EngState &S = host_states_[slot];
+    std::memset(&S, 0, sizeof(S));
+    S.status = ENG_RUNNING;
+    S.ru = 1;
+    S.init = 1;
+    S.tol2 = tol * tol;
+    S.delta2 = delta * delta;
+    S.maxiter = maxiter;
+    S.ratio2 = 1.0;
+    HW_CUDA(cudaMemsetAsync(B.y.ptr, 0, B.y.bytes, ctx_->stream));
+    HW_CUDA(cudaMemcpyAsync(d_states_.as<EngState>() + slot, &S, sizeof(S), cudaMemcpyHostToDevice, ctx_->stream));
+    // a pending reliable update computes the first residual from x
+    static const int one = 1;
+    HW_CUDA(cudaMemcpyAsync(d_ctl_.as<int>() + 2, &one, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
+    *slot_out = slot;
+    return HW_OK;
+}
+
+void Engine::release(int slot) {
+    if (slot < 0 || slot >= kEngMaxProb || !slots_[slot].used) return;
+    const int l = slots_[slot].lat;
+    EngLattice &L = tables_.lat[l];
+    int k = 0;
+    for (int q = 0; q < L.nprob; q++)
+        if (L.prob[q] != slot) L.prob[k++] = L.prob[q];
+    L.nprob = k;
+    slots_[slot].used = false;
+    host_states_[slot].status = ENG_IDLE;
+    host_states_[slot].ru = 0;
+    cudaMemcpyAsync(d_states_.as<EngState>() + slot, &host_states_[slot], sizeof(EngState), cudaMemcpyHostToDevice,
+                    ctx_->stream);
+    tables_dirty_ = true;
+}
+
+int Engine::nslots_used() const {
+    int n = 0;
+    for (int j = 0; j < kEngMaxProb; j++) n += slots_[j].used;
+    return n;
+}
+
+int Engine::upload_tables() {
+    if (!tables_dirty_) return HW_OK;
+    HW_CUDA(cudaMemcpyAsync(d_tables_.ptr, &tables_, sizeof(tables_), cudaMemcpyHostToDevice, ctx_->stream));
+    tables_dirty_ = false;
+    return HW_OK;
+}
+
+int Engine::build_graph() {
+    ptrs_.T = d_tables_.as<EngTables>();
+    ptrs_.S = d_states_.as<EngState>();
+    ptrs_.partials = d_partials_.as<double>();
+    ptrs_.tickets = d_tickets_.as<unsigned>();
+    ptrs_.ctl = d_ctl_.as<int>();
+    cudaStream_t s = ctx_->stream;
+    cudaGraph_t g = nullptr;
+    HW_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    HW_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    // chunk begin
+    HW_CUDA(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    eng_enqueue_chunk_begin(ptrs_, s);
+    cudaGraph_t tmp = nullptr;
+    HW_CUDA(cudaStreamEndCapture(s, &tmp));
+    size_t n = 0;
+    HW_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    HW_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    HW_CUDA(cudaGraphAddNode(&wnode, g, nodes.data(), nodes.size(), &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    HW_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    eng_enqueue_iteration(low_, ptrs_, grid_, s);
+    eng_enqueue_control(ptrs_, kEngMaxProb, 0, cond, 1, s);
+    HW_CUDA(cudaStreamEndCapture(s, &tmp));
+    cudaError_t e = cudaGraphInstantiate(&chunk_exec_, g, 0);
+    cudaGraphDestroy(g);
+    HW_CUDA(e);
+    return HW_OK;
+}
+
+int Engine::launch_chunk(int iters) {
+    int rc;
+    if ((rc = ensure_partials()) != HW_OK) return rc;
+    if (!chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
+    if ((rc = upload_tables()) != HW_OK) return rc;
+    // pageable source: the value is staged before the call returns
+    HW_CUDA(cudaMemcpyAsync(d_ctl_.as<int>() + 3, &iters, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
+    HW_CUDA(cudaGraphLaunch(chunk_exec_, ctx_->stream));
+    return HW_OK;
+}
+
+int Engine::read_states() {
+    HW_CUDA(cudaMemcpyAsync(pinned_states_, d_states_.ptr, sizeof(EngState) * kEngMaxProb, cudaMemcpyDeviceToHost,
+                            ctx_->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx_->stream));
+    HW_CUDA(cudaGetLastError());
+    for (int j = 0; j < kEngMaxProb; j++)
+        if (slots_[j].used) host_states_[j] = pinned_states_[j];
+    return HW_OK;
+}
+
+int get_engine(hw_context *ctx, int low, Engine **eng) {
+    HW_CHECK_ARG(low == LOW_F32 || low == LOW_F16, "engine precision must be FP32 or FP16");
+    if (!ctx->engines[low]) {
+        Engine *e = new Engine(ctx, low);
+        int rc = e->init();
+        if (rc != HW_OK) {
+            delete e;
+            return rc;
+        }
+        ctx->engines[low] = e;
+    }
+    *eng = ctx->engines[low];
+    return HW_OK;
+}
+
+void destroy_engines(hw_context *ctx) {
+    for (int k = 0; k < 3; k++) {
+        delete ctx->engines[k];
+        ctx->engines[k] = nullptr;
+    }
+}
+
+}  // namespace hw

@@ -1,0 +1,471 @@
+// Kernels of the batched mixed-precision CG engine (phase list in engine.h).
+//
+// All phases share one grid of kEngTile-thread blocks that strides over the
+// tiles of every lattice; inside a tile the block walks the lattice's active
+// slots.  Dot products are reduced per (slot, tile) with a fixed tree and
+// summed per slot in tile order by the last block to finish the lattice, so a
+// slot's arithmetic does not depend on which other slots share the launch:
+// a solve gives bitwise the same result alone and inside any batch.
+#include "engine.h"
+#include "reduce.cuh"
+#include "storage.cuh"
+
+namespace hw {
+
+namespace {
+
+template <int LOW>
+struct Low;
+
+template <>
+struct Low<LOW_F32> {
+    using Sp = SpinorF32;
+    using Lk = LinksF32x12;
+    static __device__ __forceinline__ Sp sp(void *p, float *, int stride) {
+        return Sp{static_cast<float4 *>(p), stride};
+    }
+    static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l32, L.stride}; }
+};
+
+template <>
+struct Low<LOW_F16> {
+    using Sp = SpinorF16;
+    using Lk = LinksF16x12;
+    static __device__ __forceinline__ Sp sp(void *p, float *n, int stride) {
+        return Sp{static_cast<uint4 *>(p), n, stride};
+    }
+    static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l16a, L.l16b, L.stride}; }
+};
+
+__device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
+    int l = 0;
+    const int n = T->nlat;
+    for (int k = 1; k < n; k++)
+        if (tile >= T->lat[k].tile0) l = k;
+    return l;
+}
+
+// Which slots take part in a phase.  States only change in the finishers,
+// which run after every tile of the lattice is done, so all blocks agree.
+template <int PHASE>
+__device__ __forceinline__ bool active(const EngState &s) {
+    if (PHASE >= PH_R1 && PHASE <= PH_R5) return s.ru != 0;
+    return s.status == ENG_RUNNING && s.ru == 0;
+}
+
+__device__ __forceinline__ Cx<double> ldc(const double2 *p, int stride, int c, int i) {
+    double2 v = p[(size_t)c * stride + i];
+    return {v.x, v.y};
+}
+__device__ __forceinline__ void stc(double2 *p, int stride, int c, int i, Cx<double> v) {
+    p[(size_t)c * stride + i] = make_double2(v.re, v.im);
+}
+
+// ------------------------------------------------------------------ epilogues
+
+// Low-precision phases P1..P4.  acc = (H in)(i) in FP32.
+template <int PHASE, int LOW>
+__device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st, int stride, int i,
+                                        Spinor<float> &acc, double *red) {
+    using L = Low<LOW>;
+    if (PHASE == PH_P1 || PHASE == PH_P3) {
+        L::sp(pr.t, pr.tn, stride).store(i, acc);
+    } else if (PHASE == PH_P2) {
+        const float k2 = (float)(pr.kappa * pr.kappa);
+        Spinor<float> p;
+        L::sp(pr.p, pr.pn, stride).load_cached(i, p);
+        double n2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<float> v = p.s[c / 3][c % 3] - k2 * acc.s[c / 3][c % 3];
+            acc.s[c / 3][c % 3] = v;
+            n2 += (double)norm2(v);
+        }
+        L::sp(pr.Dp, pr.Dpn, stride).store(i, acc);
+        red[0] = n2;
+    } else if (PHASE == PH_P4) {
+        const float k2 = (float)(pr.kappa * pr.kappa);
+        const float alpha = (float)st.alpha;
+        Spinor<float> d, r;
+        L::sp(pr.Dp, pr.Dpn, stride).load_cached(i, d);
+        L::sp(pr.r, pr.rn, stride).load_cached(i, r);
+        double n2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<float> ddp = d.s[c / 3][c % 3] - k2 * acc.s[c / 3][c % 3];
+            Cx<float> rv = r.s[c / 3][c % 3] - alpha * ddp;
+            r.s[c / 3][c % 3] = rv;
+            n2 += (double)norm2(rv);
+        }
+        L::sp(pr.r, pr.rn, stride).store(i, r);
+        // y += alpha p in FP32
+        Spinor<float> p, y;
+        L::sp(pr.p, pr.pn, stride).load_cached(i, p);
+        SpinorF32 ys{pr.y, stride};
+        ys.load_cached(i, y);
+#pragma unroll
+        for (int c = 0; c < 12; c++) y.s[c / 3][c % 3] = y.s[c / 3][c % 3] + alpha * p.s[c / 3][c % 3];
+        ys.store(i, y);
+        red[0] = n2;
+    }
+}
+
+// FP64 reliable-update phases R2..R5.  acc = (H in)(i) in FP64.
+template <int PHASE, int LOW>
+__device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i, Spinor<double> &acc,
+                                        double *red) {
+    const double k2 = pr.kappa * pr.kappa;
+    if (PHASE == PH_R2 || PHASE == PH_R4) {
+        SpinorF64{pr.t64, stride}.store(i, acc);
+    } else if (PHASE == PH_R3) {
+        double n2 = 0, d2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<double> mx = ldc(pr.x, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+            if (pr.mode == ENG_MODE_SOLVE) {
+                Cx<double> bv = ldc(pr.b, stride, c, i);
+                Cx<double> sv = bv - mx;
+                stc(pr.s, stride, c, i, sv);
+                n2 += norm2(sv);
+                d2 += norm2(bv);
+            } else {
+                stc(pr.s, stride, c, i, mx);
+            }
+        }
+        red[0] = n2;
+        red[1] = d2;
+    } else if (PHASE == PH_R5) {
+        double n2 = 0, d2 = 0;
+        Spinor<float> rl;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<double> v = ldc(pr.s, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+            if (pr.mode == ENG_MODE_NORMAL) {
+                Cx<double> bv = ldc(pr.b, stride, c, i);
+                v = bv - v;
+                d2 += norm2(bv);
+            }
+            n2 += norm2(v);
+            rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};
+        }
+        Low<LOW>::sp(pr.r, pr.rn, stride).store(i, rl);
+        red[0] = n2;
+        red[1] = d2;
+    }
+}
+
+// ------------------------------------------------------------------ finishers
+
+template <int PHASE>
+__device__ void finish(EngState &s, const EngProblem &pr, const double *tot, int *ctl) {
+    if (PHASE == PH_P2) {
+        s.pAp = tot[0];
+        if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
+            s.status = ENG_BREAKDOWN;
+            s.alpha = 0.0;
+        } else {
+            s.alpha = s.rr / tot[0];
+        }
+    } else if (PHASE == PH_P4) {
+        const double rr = tot[0];
+        s.iter += 1;
+        if (!isfinite(rr)) {
+            s.status = ENG_BREAKDOWN;
+            return;
+        }
+        s.rr_old = s.rr;
+        s.rr = rr;
+        s.beta = rr / s.rr_old;
+        if (rr > s.rmax2) s.rmax2 = rr;
+        // reliable update: residual fell by delta, or it looks converged, or the iterations ran out
+        const bool drop = rr < s.delta2 * s.rmax2;
+        const bool conv = pr.mode == ENG_MODE_SOLVE ? (s.ratio2 * rr <= s.tol2 * s.b2) : (rr <= s.tol2 * s.b2);
+        if (drop || conv || s.iter >= s.maxiter) {
+            s.ru = 1;
+            atomicAdd(ctl + 2, 1);
+        }
+    } else if (PHASE == PH_R3) {
+        if (pr.mode == ENG_MODE_SOLVE) {
+            s.s2 = tot[0];
+            s.b2 = tot[1];
+        }
+    } else if (PHASE == PH_R5) {
+        const double r2 = tot[0];
+        if (pr.mode == ENG_MODE_NORMAL) {
+            s.b2 = tot[1];
+            s.s2 = r2;
+        }
+        s.ru = 0;
+        s.n_ru += 1;
+        if (!isfinite(r2) || !isfinite(s.s2) || !isfinite(s.b2)) {
+            s.status = ENG_BREAKDOWN;
+            return;
+        }
+        if (s.b2 == 0.0 || s.s2 <= s.tol2 * s.b2) {
+            s.status = ENG_CONVERGED;
+            return;
+        }
+        if (s.iter >= s.maxiter) {
+            s.status = ENG_MAXITER;
+            return;
+        }
+        if (s.init) {
+            s.rr_old = r2;
+            s.beta = 0.0;
+        } else {
+            s.beta = r2 / s.rr_old;
+        }
+        s.rr = r2;
+        s.rmax2 = r2;
+        s.ratio2 = r2 > 0.0 ? s.s2 / r2 : 1.0;
+    }
+}
+
+// ------------------------------------------------------------------ hop phases
+
+template <int PHASE, int LOW>
+__global__ void __launch_bounds__(kEngTile) k_eng_hop(EngPtrs P) {
+    constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2 || PHASE == PH_R2 || PHASE == PH_R3) ? 1 : -1;
+    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R2 || PHASE == PH_R4) ? 1 : 0;
+    constexpr bool F64 = PHASE >= PH_R2 && PHASE <= PH_R5;
+    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4) ? 1 : ((PHASE == PH_R3 || PHASE == PH_R5) ? 2 : 0);
+    using L = Low<LOW>;
+    __shared__ double smem[kEngTile / 32];
+    __shared__ bool last;
+    if (PHASE >= PH_R1 && PHASE <= PH_R5 && *(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
+    const EngTables *T = P.T;
+    const int ntiles = T->ntiles;
+    const int max_tiles = T->max_tiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int l = find_lattice(T, tile);
+        const EngLattice &La = T->lat[l];
+        const Geom g = La.g;
+        const int stride = La.stride;
+        const int lt = tile - La.tile0;
+        const int i = lt * kEngTile + threadIdx.x;
+        const bool valid = i < g.Vh;
+        const int nprob = La.nprob;
+        for (int q = 0; q < nprob; q++) {
+            const int j = La.prob[q];
+            if (!active<PHASE>(P.S[j])) continue;
+            const EngProblem &pr = T->prob[j];
+            double red[2] = {0.0, 0.0};
+            if (valid) {
+                if constexpr (F64) {
+                    const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
+                    Spinor<double> acc;
+                    if (La.l64_planes == 9)
+                        hop_site<SIGN>(g, OUTPAR, i, SpinorF64{const_cast<double2 *>(in), stride},
+                                       LinksF64x18{La.l64, stride}, acc);
+                    else
+                        hop_site<SIGN>(g, OUTPAR, i, SpinorF64{const_cast<double2 *>(in), stride},
+                                       LinksF64x12{La.l64, stride}, acc);
+                    epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
+                } else {
+                    void *in = (PHASE == PH_P1) ? pr.p : (PHASE == PH_P3 ? pr.Dp : pr.t);
+                    float *inn = (PHASE == PH_P1) ? pr.pn : (PHASE == PH_P3 ? pr.Dpn : pr.tn);
+                    Spinor<float> acc;
+                    hop_site<SIGN>(g, OUTPAR, i, L::sp(in, inn, stride), L::lk(La), acc);
+                    epi_low<PHASE, LOW>(pr, P.S[j], stride, i, acc, red);
+                }
+            }
+            if constexpr (NRED > 0) {
+#pragma unroll
+                for (int k = 0; k < NRED; k++) {
+                    double s = block_sum<kEngTile>(red[k], smem);
+                    if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = s;
+                }
+            }
+        }
+        if constexpr (NRED > 0) {
+            if (threadIdx.x == 0) {
+                __threadfence();
+                unsigned t = atomicAdd(P.tickets + l, 1u);
+                last = (t == (unsigned)La.ntiles - 1u);
+            }
+            __syncthreads();
+            if (last) {
+                __threadfence();
+                const int nt = La.ntiles;
+                for (int q = 0; q < nprob; q++) {
+                    const int j = La.prob[q];
+                    if (!active<PHASE>(P.S[j])) continue;
+                    double tot[2] = {0.0, 0.0};
+#pragma unroll
+                    for (int k = 0; k < NRED; k++) {
+                        const double *pp = P.partials + ((size_t)j * 2 + k) * max_tiles;
+                        double s = 0.0;
+                        for (int t2 = threadIdx.x; t2 < nt; t2 += kEngTile) s += __ldcg(pp + t2);
+                        tot[k] = block_sum<kEngTile>(s, smem);
+                    }
+                    if (threadIdx.x == 0) finish<PHASE>(P.S[j], T->prob[j], tot, P.ctl);
+                    __syncthreads();
+                }
+                if (threadIdx.x == 0) P.tickets[l] = 0u;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ vector phases
+
+// R1: x += y; y = 0 (slots with a pending reliable update)
+// P5: p = r + beta p, or p = r on a slot's first iteration (running slots)
+template <int PHASE, int LOW>
+__global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
+    using L = Low<LOW>;
+    if (PHASE == PH_R1 && *(volatile int *)(P.ctl + 2) == 0) return;
+    const EngTables *T = P.T;
+    const int ntiles = T->ntiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int l = find_lattice(T, tile);
+        const EngLattice &La = T->lat[l];
+        const int stride = La.stride;
+        const int i = (tile - La.tile0) * kEngTile + threadIdx.x;
+        if (i >= La.g.Vh) continue;
+        for (int q = 0; q < La.nprob; q++) {
+            const int j = La.prob[q];
+            const EngState &s = P.S[j];
+            if (!active<PHASE>(s)) continue;
+            const EngProblem &pr = T->prob[j];
+            if (PHASE == PH_R1) {
+                SpinorF32 ys{pr.y, stride};
+                Spinor<float> y;
+                ys.load_cached(i, y);
+#pragma unroll
+                for (int c = 0; c < 12; c++) {
+                    Cx<double> xv = ldc(pr.x, stride, c, i);
+                    xv.re += (double)y.s[c / 3][c % 3].re;
+                    xv.im += (double)y.s[c / 3][c % 3].im;
+                    stc(pr.x, stride, c, i, xv);
+                    y.s[c / 3][c % 3] = {0.f, 0.f};
+                }
+                ys.store(i, y);
+            } else {
+                Spinor<float> r, p;
+                L::sp(pr.r, pr.rn, stride).load_cached(i, r);
+                if (s.init) {
+                    L::sp(pr.p, pr.pn, stride).store(i, r);
+                } else {
+                    const float beta = (float)s.beta;
+                    L::sp(pr.p, pr.pn, stride).load_cached(i, p);
+#pragma unroll
+                    for (int c = 0; c < 12; c++) p.s[c / 3][c % 3] = r.s[c / 3][c % 3] + beta * p.s[c / 3][c % 3];
+                    L::sp(pr.p, pr.pn, stride).store(i, p);
+                }
+            }
+        }
+    }
+}
+
+// One block: end of an iteration.  Clears the first-iteration flags, counts
+// running slots, and keeps the chunk's WHILE loop going while some slot runs
+// and fewer than `chunk` iterations ran.  No waiting: the loop is bounded by
+// `chunk` and by every slot's maxiter.
+__global__ void k_eng_control(EngPtrs P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond) {
+    __shared__ int running;
+    if (threadIdx.x == 0) running = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < nprob; j += blockDim.x) {
+        EngState &s = P.S[j];
+        if (s.status == ENG_RUNNING && s.ru == 0 && s.init) s.init = 0;
+        if (s.status == ENG_RUNNING) atomicAdd(&running, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (chunk <= 0) chunk = P.ctl[3];
+        const int it = P.ctl[0] + 1;
+        P.ctl[0] = it;
+        P.ctl[1] = running;
+        P.ctl[2] = 0;  // pending reliable updates were served this iteration
+        if (use_cond) cudaGraphSetConditional(h, (running > 0 && it < chunk) ? 1u : 0u);
+    }
+}
+
+__global__ void k_eng_chunk_begin(EngPtrs P) { P.ctl[0] = 0; }
+
+// FP64 link planes (first six elements = rows 0 and 1) -> FP32 / FP16 12-real planes
+__global__ void k_eng_links(Geom g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
+                            uint2 *l16b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int pd = blockIdx.y;  // parity*4 + dir
+    if (i >= g.Vh) return;
+    float e[12];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double2 v = l64[((size_t)pd * planes + k) * stride + i];
+        e[2 * k] = (float)v.x;
+        e[2 * k + 1] = (float)v.y;
+    }
+    if (l32) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            l32[((size_t)pd * 3 + k) * stride + i] = make_float4(e[4 * k], e[4 * k + 1], e[4 * k + 2], e[4 * k + 3]);
+    }
+    if (l16a) {
+        uint4 a;
+        uint2 b;
+        __half2 *ha = reinterpret_cast<__half2 *>(&a);
+        __half2 *hb = reinterpret_cast<__half2 *>(&b);
+#pragma unroll
+        for (int k = 0; k < 4; k++) ha[k] = __floats2half2_rn(e[2 * k], e[2 * k + 1]);
+#pragma unroll
+        for (int k = 0; k < 2; k++) hb[k] = __floats2half2_rn(e[8 + 2 * k], e[9 + 2 * k]);
+        l16a[(size_t)pd * stride + i] = a;
+        l16b[(size_t)pd * stride + i] = b;
+    }
+}
+
+template <int LOW>
+void enqueue_iteration_t(const EngPtrs &P, int grid, int grid64, cudaStream_t s) {
+    k_eng_hop<PH_P1, LOW><<<grid, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_P2, LOW><<<grid, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_P3, LOW><<<grid, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_P4, LOW><<<grid, kEngTile, 0, s>>>(P);
+    k_eng_vec<PH_R1, LOW><<<grid, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_R2, LOW><<<grid64, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_R3, LOW><<<grid64, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_R4, LOW><<<grid64, kEngTile, 0, s>>>(P);
+    k_eng_hop<PH_R5, LOW><<<grid64, kEngTile, 0, s>>>(P);
+    k_eng_vec<PH_P5, LOW><<<grid, kEngTile, 0, s>>>(P);
+}
+
+}  // namespace
+
+void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    if (low == LOW_F16)
+        enqueue_iteration_t<LOW_F16>(P, G.low, G.f64, s);
+    else
+        enqueue_iteration_t<LOW_F32>(P, G.low, G.f64, s);
+}
+
+void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
+                         cudaStream_t s) {
+    k_eng_control<<<1, 64, 0, s>>>(P, nprob, chunk, h, use_cond);
+}
+
+void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s) { k_eng_chunk_begin<<<1, 1, 0, s>>>(P); }
+
+void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
+                       uint2 *l16b, cudaStream_t s) {
+    dim3 grid((g.Vh + 255) / 256, 8);
+    k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b);
+}
+
+EngGrid eng_grid_size(int low) {
+    int dev = 0, sms = 148, lo = 0, hi = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (low == LOW_F16)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_hop<PH_P4, LOW_F16>, kEngTile, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_hop<PH_P4, LOW_F32>, kEngTile, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hi, k_eng_hop<PH_R5, LOW_F32>, kEngTile, 0);
+    EngGrid G;
+    G.low = sms * (lo < 1 ? 1 : lo);
+    G.f64 = sms * (hi < 1 ? 1 : hi);
+    return G;
+}
+
+}  // namespace hw

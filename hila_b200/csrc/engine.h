@@ -1,0 +1,131 @@
+// Batched mixed-precision CG engine: device tables shared by engine.cu and engine.cpp.
+//
+// An engine holds up to kEngMaxLat lattices (each with its gauge field) and up
+// to kEngMaxProb solve slots.  Every phase of a CG iteration is ONE launch of a
+// persistent-style grid that walks the tiles (kEngTile sites) of all lattices,
+// and inside each tile every active slot on that lattice, so links loaded for
+// the first right-hand side are re-read from L1/L2 by the others.  The slot
+// states live in device memory; the kernels read the tables through a pointer,
+// so the same captured CUDA graph serves every batch composition.
+//
+// Inner iteration (low precision: FP32, or FP16 with a per-site scale; links
+// 12 reals; accumulation in FP32; dot products in FP64):
+//   P1  t  = H^{oe}_+ p
+//   P2  Dp = p - kappa^2 H^{eo}_+ t           |Dp|^2 -> alpha
+//   P3  t  = H^{oe}_- Dp
+//   P4  DDp = Dp - kappa^2 H^{eo}_- t; r -= alpha DDp; y += alpha p (FP32)
+//                                              |r|^2 -> beta, reliable-update decision
+// Reliable update (FP64, only slots that asked for it):
+//   R1  x += y; y = 0                          (FP64 solution accumulation)
+//   R2  t64 = H^{oe}_+ x
+//   R3  solve mode:  s = b - (x - kappa^2 H t64)   |s|^2, |b|^2
+//       normal mode: s = x - kappa^2 H t64         (= M x)
+//   R4  t64 = H^{oe}_- s
+//   R5  solve mode:  r = s - kappa^2 H^dag t64      (= M^dag (b - M x))
+//       normal mode: r = b - (s - kappa^2 H^dag t64) (= b - M^dag M x), |b|^2
+//       r_low = r, |r|^2 -> true residual, convergence, beta
+//   P5  p = r + beta p   (p = r on a slot's first iteration)
+#pragma once
+
+#include "kernels.h"
+
+namespace hw {
+
+constexpr int kEngTile = 128;      // sites per tile = threads per block of the engine kernels
+constexpr int kEngMaxLat = 32;     // lattices per engine
+constexpr int kEngMaxProb = 64;    // solve slots per engine
+constexpr int kEngMaxRhs = 16;     // slots per lattice
+
+enum EngStatus : int { ENG_RUNNING = 0, ENG_CONVERGED = 1, ENG_MAXITER = 2, ENG_BREAKDOWN = 3, ENG_IDLE = 4 };
+enum EngMode : int { ENG_MODE_SOLVE = 0, ENG_MODE_NORMAL = 1 };
+
+struct EngLattice {
+    Geom g;
+    int stride;       // padded sites per parity of every field of this lattice
+    int tile0;        // first global tile
+    int ntiles;       // tiles of one parity
+    int nprob;        // slots on this lattice
+    int prob[kEngMaxRhs];
+    // links: FP64 (18 or 12 reals) for the reliable updates, low precision for the inner solve
+    const double2 *l64;
+    int l64_planes;
+    const float4 *l32;   // FP32, 12 reals: 3 float4 planes per (parity, dir)
+    const uint4 *l16a;   // FP16, 12 reals: 8 halves ...
+    const uint2 *l16b;   // ... + 4 halves per link
+};
+
+struct EngProblem {
+    int lat;
+    int mode;
+    double kappa;
+    // low precision (EVEN: p, r, Dp; ODD: t); FP16 fields carry a norm plane
+    void *p, *r, *Dp, *t;
+    float *pn, *rn, *Dpn, *tn;
+    float4 *y;  // FP32 solution increment since the last reliable update (6 float4 planes)
+    // FP64 (EVEN: x, b, s; ODD: t64)
+    double2 *x, *b, *s, *t64;
+};
+
+struct EngState {
+    double rr;       // |r|^2 (iterated, or true after a reliable update)
+    double rr_old;   // |r|^2 of the previous iteration (beta after a reliable update)
+    double pAp;
+    double alpha, beta;
+    double rmax2;    // largest |r|^2 since the last reliable update
+    double b2;       // |b|^2 of the system being solved
+    double s2;       // |b - M x|^2 (solve mode) at the last reliable update
+    double ratio2;   // s2 / rr at the last reliable update: estimates |b - M x| from |r|
+    double tol2;     // accuracy^2
+    double delta2;   // reliable-update factor^2
+    double seconds;  // unused by the device; host bookkeeping
+    int iter, maxiter;
+    int status;      // EngStatus
+    int ru;          // 1: reliable update pending
+    int init;        // 1: first reliable update (r from x), p = r afterwards
+    int n_ru;
+    int pad[2];
+};
+
+struct EngTables {
+    int nlat;
+    int ntiles;  // total tiles over all lattices
+    int max_tiles;  // partial-sum stride: largest ntiles of any lattice
+    int pad;
+    EngLattice lat[kEngMaxLat];
+    EngProblem prob[kEngMaxProb];
+};
+
+// device pointers the engine kernels take
+struct EngPtrs {
+    const EngTables *T;
+    EngState *S;
+    double *partials;     // kEngMaxProb * 2 * max_tiles
+    unsigned *tickets;    // one per lattice
+    int *ctl;             // [0] iterations run in this chunk, [1] running slots,
+                          // [2] reliable updates requested in this iteration,
+                          // [3] iteration limit of a chunk (control kernel with chunk <= 0)
+};
+
+struct EngGrid {
+    int low;  // blocks of the low-precision phases (all SMs x resident blocks)
+    int f64;  // blocks of the FP64 reliable-update phases
+};
+
+enum EngPhase : int { PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R5, PH_P5 };
+
+// low-precision format of one engine (template parameter of the inner phases)
+enum EngLow : int { LOW_F32 = 1, LOW_F16 = 2 };
+
+// Enqueue one CG iteration (all phases) on stream s.
+void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s);
+// While-loop control: counts running slots, stops after `chunk` iterations or when none runs.
+void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
+                         cudaStream_t s);
+void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s);
+// Convert FP64 link planes to the 12-real FP32 / FP16 planes of the inner solve.
+void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
+                       uint2 *l16b, cudaStream_t s);
+// grid sizes (blocks) of the engine kernels on the current device
+EngGrid eng_grid_size(int low);
+
+}  // namespace hw

@@ -1,0 +1,84 @@
+// Host side of the batched mixed-precision CG engine (kernels in engine.cu).
+#pragma once
+
+#include <vector>
+
+#include "engine.h"
+#include "hw_internal.h"
+
+namespace hw {
+
+// Device buffers of one solve slot, sized for a lattice stride.
+struct SlotBuffers {
+    DevBuf p, r, Dp, t, pn, rn, Dpn, tn, y, s, t64;
+    DevBuf x_own, b_own;  // FP64 EVEN halves for slots that own their source / solution
+    int stride = 0;
+};
+
+struct SlotInfo {
+    bool used = false;
+    int lat = -1;
+};
+
+class Engine {
+  public:
+    Engine(hw_context *ctx, int low) : ctx_(ctx), low_(low) {}
+    ~Engine();
+    int init();
+    int low() const { return low_; }
+
+    // index of the lattice of `gauge` in this engine, adding it if needed
+    int lattice_index(const hw_gauge *gauge, int *idx);
+    // drop lattices with no used slot (compacts the tile list)
+    int prune_lattices();
+    int free_slots_on(int lat) const;
+
+    // Start a solve in a free slot.  b, x: FP64 EVEN halves (stride of the
+    // lattice); null means slot-owned buffers (filled with upload_b / read with x_ptr).
+    int admit(int lat, double kappa, double2 *b, double2 *x, double tol, int maxiter, double delta, int mode,
+              int *slot);
+    double2 *own_b(int slot) { return bufs_[slot].b_own.as<double2>(); }
+    double2 *own_x(int slot) { return bufs_[slot].x_own.as<double2>(); }
+    int ensure_own(int slot);
+    // stream-ordered: run up to `iters` iterations of every running slot
+    // (stops early when none runs)
+    int launch_chunk(int iters);
+    // copy the slot states to the host mirror (synchronises the stream)
+    int read_states();
+    const EngState &state(int slot) const { return host_states_[slot]; }
+    void release(int slot);
+    int nslots_used() const;
+    size_t slot_bytes(int lat) const;
+    const EngLattice &lattice(int l) const { return tables_.lat[l]; }
+    int nlat() const { return tables_.nlat; }
+    const hw_gauge *gauge(int l) const { return gauges_[l]; }
+    int upload_tables();
+
+  private:
+    int ensure_slot_buffers(int slot, int stride);
+    int build_graph();
+    int ensure_partials();
+
+    hw_context *ctx_;
+    int low_;
+    bool ready_ = false;
+    EngTables tables_{};
+    std::vector<const hw_gauge *> gauges_;
+    SlotInfo slots_[kEngMaxProb];
+    SlotBuffers bufs_[kEngMaxProb];
+    EngState host_states_[kEngMaxProb];
+    EngState *pinned_states_ = nullptr;
+    DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_;
+    size_t partial_tiles_ = 0;
+    EngGrid grid_{};
+    EngPtrs ptrs_{};
+    cudaGraphExec_t chunk_exec_ = nullptr;
+    bool tables_dirty_ = true;
+};
+
+// per-context engine for a low precision (LOW_F32 / LOW_F16), created on first use
+int get_engine(hw_context *ctx, int low, Engine **eng);
+// make the FP32 / FP16 link copies of a gauge field
+int ensure_low_links(const hw_gauge *G, int low);
+
+}  // namespace hw

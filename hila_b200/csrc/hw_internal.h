@@ -15,6 +15,8 @@
 
 namespace hw {
 
+class Engine;
+
 // ------------------------------------------------------------------ errors
 
 void set_error(const char *fmt, ...);
@@ -75,6 +77,7 @@ struct hw_context {
         return hw::RedBuf{red_partials.as<double>(), red_ticket.as<unsigned>()};
     }
     size_t red_capacity_doubles = 0;
+    hw::Engine *engines[3] = {nullptr, nullptr, nullptr};  // batched mixed-precision engines by precision
 };
 
 // FP64 half-lattice field buffer
@@ -117,6 +120,7 @@ struct hw_lattice {
     hw::Geom g{};
     std::unique_ptr<CgWorkspace> ws;
     hw_field *host_b = nullptr, *host_x = nullptr;  // fields behind the host-array solve
+    bool tuned = false;  // FP64 hop launch shape chosen (g.hop_variant)
     ~hw_lattice();
 };
 
@@ -126,7 +130,7 @@ struct hw_gauge {
     hw::DevBuf f64;  // FP64 planes
     hw::GaugeF64 U() const { return hw::GaugeF64{f64.as<double2>(), lat->stride, link_format == 12 ? 6 : 9}; }
     // low-precision copies for mixed-precision solves (built on first use)
-    hw::DevBuf f32, f16a, f16b;
+    mutable hw::DevBuf f32, f16a, f16b;
 };
 
 struct hw_field {
@@ -138,4 +142,7 @@ namespace hw {
 int ensure_workspace(hw_lattice *lat);
 int ensure_reduction_capacity(hw_context *ctx, long nblocks);
 int ensure_stage(hw_context *ctx, size_t bytes);
+// pick the fastest FP64 hop launch shape for this lattice once (HW_HOP_VARIANT overrides)
+int tune_hop(hw_lattice *lat, const hw_gauge *G);
+void destroy_engines(hw_context *ctx);
 }  // namespace hw

@@ -280,6 +280,7 @@ static int solve_common(const hw_gauge *G, double kappa, const hw_field *in, hw_
     HW_CUDA(cudaSetDevice(ctx->device));
     if (P.precision != HW_PREC_F64) return mixed_solve(G, kappa, in, out, mode, P, result);
     if ((rc = ensure_workspace(lat)) != HW_OK) return rc;
+    if ((rc = tune_hop(lat, G)) != HW_OK) return rc;
     F64Solve S;
     S.ctx = ctx;
     S.lat = lat;

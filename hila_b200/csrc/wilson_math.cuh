@@ -226,6 +226,7 @@ struct Geom {
     int Vh;         // sites per parity
     int sy, sz, st; // checkerboard strides of y, z, t: lxh, lxh*Ly, lxh*Ly*Lz
     int tap;        // 1: fermion values crossing the t boundary are negated
+    int hop_variant;  // launch shape of the FP64 hop kernels (host-side choice, see dslash_f64.cu)
 };
 
 struct SiteNbrs {

@@ -176,6 +176,29 @@ int hw_wilson_evenodd_solve(const hw_gauge *gauge, double kappa, const hw_field 
 int hw_wilson_evenodd_solve_host(const hw_gauge *gauge, double kappa, const double *b_host, double *x_host,
                                  const hw_cg_params *params, hw_cg_result *result);
 
+/* ------------------------------------------------------------------ batches */
+
+/* One solve of M x = b (EVEN sites) inside a batch. */
+typedef struct hw_solve_request {
+    const hw_gauge *gauge; /* gauge field (selects the lattice) */
+    double kappa;
+    const hw_field *b;     /* right-hand side */
+    hw_field *x;           /* solution; holds the initial guess on entry */
+    double accuracy;       /* stop when |b - M x| / |b| <= accuracy (FP64, recomputed) */
+    int maxiters;
+} hw_solve_request;
+
+/* Many right-hand sides on many lattices at once (no reference counterpart:
+ * HILA solves one source per CG<Op>::apply call).  Mixed precision (FP32, or
+ * FP16 with per-site scale) inner CG with FP64 reliable updates, solution
+ * accumulation and dot products; `delta` is the reliable-update factor
+ * (<= 0: 0.1).  Every CG phase of all admitted solves runs in one kernel
+ * launch; up to 16 solves per lattice and 64 in total run at a time, the rest
+ * are admitted as earlier ones finish.  results[k] receives request k's
+ * outcome; each solve gives bitwise the same result alone and in a batch. */
+int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_request *requests, int n,
+                   hw_cg_result *results);
+
 /* ------------------------------------------------------------------ inputs */
 
 /* Seeded synthetic inputs (no reference counterpart beyond hila::seed_random

@@ -1,0 +1,119 @@
+"""GPU tests of the mixed-precision solves and of the batched engine.
+
+Every solve is judged by its true residual |b - M x| / |b| recomputed by the
+CPU oracle in FP64: <= 1e-10.  Batched solves must give bitwise the same
+solution alone and inside a batch.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def make(hw, ctx, oracle, dims, seed, link_format=18):
+    U = oracle.gen_links(dims, 0.3, seed)
+    lat = hw.Lattice(ctx, dims, True)
+    return U, lat, hw.GaugeField(lat, U, link_format)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+@pytest.mark.parametrize("dims,kappa,link_format", [((8, 8, 8, 8), 0.12, 18), ((16, 8, 8, 16), 0.124, 12),
+                                                    ((2, 4, 6, 8), 0.115, 18)])
+def test_mixed_solve(hw, ctx, oracle, precision, dims, kappa, link_format):
+    U, lat, G = make(hw, ctx, oracle, dims, 11, link_format)
+    b = oracle.gen_spinor(dims, 12, oracle.EVEN)
+    D = hw.Dirac_Wilson_evenodd(kappa, G)
+    fb, fx = hw.Field(lat, b), hw.Field(lat)
+    res = D.solve(fb, fx, accuracy=TOL, precision=precision)
+    assert res.converged, res
+    assert res.reliable_updates >= 2
+    x = fx.download()
+    tr = oracle.true_residual(dims, U, kappa, b, x)
+    assert tr <= TOL
+    assert abs(tr - res.true_residual) <= 1e-3 * tr + 1e-15
+    # the FP64 solve agrees to the accuracy the condition number allows
+    fx64 = hw.Field(lat)
+    r64 = D.solve(fb, fx64, accuracy=TOL)
+    x64 = fx64.download()
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_mixed_normal_equations(hw, ctx, oracle, precision):
+    """CG<Op>::apply semantics in mixed precision: M^dag M x = in to 1e-10 (true)."""
+    dims = (8, 8, 8, 8)
+    U, lat, G = make(hw, ctx, oracle, dims, 21)
+    src = oracle.gen_spinor(dims, 22, oracle.EVEN)
+    D = hw.Dirac_Wilson_evenodd(0.12, G)
+    fin, fout = hw.Field(lat, src), hw.Field(lat)
+    res = hw.CG(D, accuracy=TOL, precision=precision).apply(fin, fout)
+    assert res.converged, res
+    assert oracle.true_residual_normal(dims, U, 0.12, src, fout.download()) <= TOL
+
+
+def test_mixed_edge_cases(hw, ctx, oracle):
+    dims = (4, 4, 4, 4)
+    U, lat, G = make(hw, ctx, oracle, dims, 31)
+    D = hw.Dirac_Wilson_evenodd(0.12, G)
+    fb, fx = hw.Field(lat), hw.Field(lat)
+    res = D.solve(fb, fx, precision="f16")
+    assert res.converged and res.iterations == 0 and not fx.download().any()
+    b = oracle.gen_spinor(dims, 32, oracle.EVEN)
+    fb.upload(b)
+    res = D.solve(fb, fx, accuracy=TOL, maxiters=3, precision="f16")
+    assert res.status == hw.HW_ERR_NOT_CONVERGED and res.iterations == 3
+    bad = b.copy()
+    bad[5, 1, 1, 1] = np.inf
+    fb.upload(bad)
+    fx.zero()
+    res = D.solve(fb, fx, precision="f32")
+    assert res.status == hw.HW_ERR_BREAKDOWN
+    fb.upload(b)
+    fx.zero()
+    assert D.solve(fb, fx, accuracy=TOL, precision="f32").converged
+
+
+@pytest.mark.parametrize("precision", ["f16", "f32"])
+def test_batch_uneven_lattices(hw, ctx, oracle, precision):
+    """Several lattices of uneven volume, several right-hand sides each, in one batch."""
+    specs = [((8, 8, 8, 8), 41, [0.115, 0.12, 0.124]), ((4, 4, 4, 8), 42, [0.12, 0.118]),
+             ((6, 4, 4, 4), 43, [0.121]), ((8, 8, 4, 8), 44, [0.116, 0.124, 0.119, 0.12])]
+    reqs, checks = [], []
+    keep = []
+    for dims, seed, kappas in specs:
+        U, lat, G = make(hw, ctx, oracle, dims, seed)
+        keep += [lat, G]
+        for n, kappa in enumerate(kappas):
+            b = oracle.gen_spinor(dims, 1000 * seed + n, oracle.EVEN)
+            fb, fx = hw.Field(lat, b), hw.Field(lat)
+            D = hw.Dirac_Wilson_evenodd(kappa, G)
+            reqs.append((D, fb, fx, TOL))
+            checks.append((dims, U, kappa, b, fx, D, fb))
+    results = hw.batch_solve(ctx, reqs, precision=precision)
+    for (dims, U, kappa, b, fx, D, fb), r in zip(checks, results):
+        assert r.converged, r
+        assert oracle.true_residual(dims, U, kappa, b, fx.download()) <= TOL
+    # the same request alone gives bitwise the same solution
+    dims, U, kappa, b, fx, D, fb = checks[1]
+    fx2 = hw.Field(D.gauge.lattice)
+    r2 = hw.batch_solve(ctx, [(D, fb, fx2, TOL)], precision=precision)[0]
+    assert r2.iterations == results[1].iterations
+    assert np.array_equal(fx2.download(), fx.download())
+
+
+def test_batch_refills_slots(hw, ctx, oracle):
+    """More right-hand sides than one lattice's 16 slots: later ones are admitted as slots free up."""
+    dims = (4, 4, 4, 4)
+    U, lat, G = make(hw, ctx, oracle, dims, 51)
+    reqs, bs = [], []
+    for n in range(20):
+        b = oracle.gen_spinor(dims, 5100 + n, oracle.EVEN)
+        D = hw.Dirac_Wilson_evenodd(0.115 + 0.0005 * (n % 10), G)
+        reqs.append((D, hw.Field(lat, b), hw.Field(lat), TOL))
+        bs.append(b)
+    results = hw.batch_solve(ctx, reqs, precision="f16")
+    for (D, fb, fx, _), b, r in zip(reqs, bs, results):
+        assert r.converged
+        assert oracle.true_residual(dims, U, D.kappa, b, fx.download()) <= TOL
