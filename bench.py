@@ -262,7 +262,8 @@ def run_ours(args, dist: Dist):
         def batch_once():
             for f in fxs:
                 f.zero()
-            return hw.batch_solve(ctx, [(D, fbs[k], fxs[k], w["tol"]) for k in range(nrhs)], precision=prec)
+            return hw.batch_solve(ctx, [(D, fbs[k], fxs[k], w["tol"]) for k in range(nrhs)], precision=prec,
+                                  delta=args.delta)
 
         for _ in range(args.warmup):
             batch_once()
@@ -314,7 +315,8 @@ def run_ours(args, dist: Dist):
     else:
         def solve_once():
             fx.zero()
-            return D.solve(fb, fx, accuracy=w["tol"], precision=args.precision, use_graph=not args.no_graph)
+            return D.solve(fb, fx, accuracy=w["tol"], precision=args.precision, use_graph=not args.no_graph,
+                           delta=args.delta)
 
         for _ in range(args.warmup):
             r = solve_once()
@@ -439,8 +441,11 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
     ap.add_argument("--link-format", type=int, default=18, choices=[18, 12])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-graph", action="store_true", help="FP64 CG iterations from a host loop (for launch lists)")
+    ap.add_argument("--no-graph", action="store_true", help="CG iterations from a host loop (for launch lists)")
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update factor of the mixed-precision solves")
     args = ap.parse_args()
+    if args.no_graph:
+        os.environ["HW_USE_GRAPH"] = "0"
     if args.warmup < 3:
         args.warmup = 3
     dist = Dist()

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine_host.h"
@@ -55,6 +56,9 @@ int Engine::init() {
     }
     HW_CUDA(cudaMemcpyAsync(d_states_.ptr, host_states_, sizeof(host_states_), cudaMemcpyHostToDevice, ctx_->stream));
     grid_ = eng_grid_size(low_);
+    // HW_USE_GRAPH=0 runs the iterations from a host loop instead of the captured
+    // WHILE graph (profilers see the individual kernel launches)
+    if (const char *env = std::getenv("HW_USE_GRAPH")) use_graph_ = std::atoi(env) != 0;
     if ((rc = ensure_partials()) != HW_OK) return rc;
     ready_ = true;
     return HW_OK;
@@ -285,12 +289,16 @@ int Engine::upload_tables() {
     return HW_OK;
 }
 
-int Engine::build_graph() {
+void Engine::set_ptrs() {
     ptrs_.T = d_tables_.as<EngTables>();
     ptrs_.S = d_states_.as<EngState>();
     ptrs_.partials = d_partials_.as<double>();
     ptrs_.tickets = d_tickets_.as<unsigned>();
     ptrs_.ctl = d_ctl_.as<int>();
+}
+
+int Engine::build_graph() {
+    set_ptrs();
     cudaStream_t s = ctx_->stream;
     cudaGraph_t g = nullptr;
     HW_CUDA(cudaGraphCreate(&g, 0));
@@ -325,8 +333,18 @@ int Engine::build_graph() {
 int Engine::launch_chunk(int iters) {
     int rc;
     if ((rc = ensure_partials()) != HW_OK) return rc;
-    if (!chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
+    if (use_graph_ && !chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
     if ((rc = upload_tables()) != HW_OK) return rc;
+    if (!use_graph_) {
+        set_ptrs();
+        eng_enqueue_chunk_begin(ptrs_, ctx_->stream);
+        for (int k = 0; k < iters; k++) {
+            eng_enqueue_iteration(low_, ptrs_, grid_, ctx_->stream);
+            eng_enqueue_control(ptrs_, kEngMaxProb, iters, 0, 0, ctx_->stream);
+        }
+        HW_CUDA(cudaGetLastError());
+        return HW_OK;
+    }
     // pageable source: the value is staged before the call returns
     HW_CUDA(cudaMemcpyAsync(d_ctl_.as<int>() + 3, &iters, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
     HW_CUDA(cudaGraphLaunch(chunk_exec_, ctx_->stream));

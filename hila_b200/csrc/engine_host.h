@@ -57,6 +57,7 @@ class Engine {
   private:
     int ensure_slot_buffers(int slot, int stride);
     int build_graph();
+    void set_ptrs();
     int ensure_partials();
 
     hw_context *ctx_;
@@ -74,6 +75,7 @@ class Engine {
     EngPtrs ptrs_{};
     cudaGraphExec_t chunk_exec_ = nullptr;
     bool tables_dirty_ = true;
+    bool use_graph_ = true;
 };
 
 // per-context engine for a low precision (LOW_F32 / LOW_F16), created on first use
