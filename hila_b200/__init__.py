@@ -111,6 +111,8 @@ _SIGNATURES = {
                                                ctypes.POINTER(_CgResult)]),
     "hw_wilson_evenodd_solve_host": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp, ctypes.POINTER(_CgParams),
                                                     ctypes.POINTER(_CgResult)]),
+    "hw_wilson_evenodd_apply_noalloc": (ctypes.c_int, [_ip, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp,
+                                                       ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
     "hw_batch_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_SolveRequest),
                                       ctypes.c_int, ctypes.POINTER(_CgResult)]),
     "hw_generate_links": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_uint64, _dp]),
@@ -466,3 +468,16 @@ def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0
     if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
         _check(rc)
     return [CGResult.from_c(res[k]) for k in range(n)]
+
+
+def wilson_evenodd_apply_noalloc(dims, kappa: float, sign: int, links_ptr: int, in_ptr: int, out_ptr: int,
+                                 stride: int, link_format: int = 18, antiperiodic: bool = True,
+                                 stream: int = 0) -> None:
+    """hw_wilson_evenodd_apply_noalloc on raw device pointers (even-odd layout).
+
+    Allocates no device memory: for callers that cannot allocate.  At most
+    32768 sites per parity; stream-ordered on `stream`.
+    """
+    _check(lib().hw_wilson_evenodd_apply_noalloc(_dims(dims), int(bool(antiperiodic)), float(kappa), int(sign),
+                                                 _vp(links_ptr), int(link_format), _vp(in_ptr), _vp(out_ptr),
+                                                 int(stride), _vp(stream)))

@@ -128,6 +128,26 @@ int hw_wilson_apply(const hw_gauge *gauge, double kappa, int sign, const hw_fiel
 int hw_wilson_hop(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out, int parity, int sign,
                   int set);
 
+/* Even-odd operator that allocates no device memory (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc -- code running while a
+ * framework owns device memory through its own pool, code inside regions where
+ * an allocation (which synchronises the device) is not allowed, hosts that
+ * preallocate everything up front.  Computes out_e = M_sign in_e like
+ * hw_wilson_evenodd_apply (sign +1 apply, -1 dagger) from device arrays in the
+ * library's even-odd layout: links = ((parity*4 + dir)*planes + k)*stride + i
+ * double2 planes (planes 9 for link_format 18, 6 for 12); in_even / out_even =
+ * 12 double2 planes of `stride` sites (component 3*spin + colour).  The odd
+ * temporary comes from a fixed 6 MiB device array inside the library, so the
+ * lattice may have at most 32768 sites per parity (a 16^4 lattice); larger
+ * lattices are rejected with HW_ERR_INVALID.  Stream-ordered on `stream`
+ * (a cudaStream_t, NULL = default stream) of the current device.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU (other streams or threads on the same device) race. */
+int hw_wilson_evenodd_apply_noalloc(const int dims[4], int t_antiperiodic, double kappa, int sign,
+                                    const double *links, int link_format, const double *in_even, double *out_even,
+                                    int stride, void *stream);
+
 /* ------------------------------------------------------------------ solver */
 
 typedef struct hw_cg_params {
