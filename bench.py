@@ -443,7 +443,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="CG iterations from a host loop (for launch lists)")
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update factor of the mixed-precision solves")
+    ap.add_argument("--lattice", default=None, help="override the workload's lattice, e.g. 24x24x24x24")
+    ap.add_argument("--nrhs", type=int, default=None, help="override the right-hand sides per step (mrhs)")
     args = ap.parse_args()
+    if args.lattice:
+        WORKLOADS[args.workload]["dims"] = tuple(int(v) for v in args.lattice.split("x"))
+    if args.nrhs:
+        WORKLOADS[args.workload]["nrhs"] = args.nrhs
     if args.no_graph:
         os.environ["HW_USE_GRAPH"] = "0"
     if args.warmup < 3:

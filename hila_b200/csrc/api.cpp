@@ -195,14 +195,7 @@ int hw_lattice_create(hw_context *ctx, const int dims[4], int t_antiperiodic, hw
     l->V = V;
     l->Vh = V / 2;
     l->stride = padded_stride(l->Vh);
-    Geom &g = l->g;
-    for (int d = 0; d < 4; d++) g.L[d] = dims[d];
-    g.lxh = dims[0] / 2;
-    g.Vh = (int)l->Vh;
-    g.sy = g.lxh;
-    g.sz = g.lxh * dims[1];
-    g.st = g.lxh * dims[1] * dims[2];
-    g.tap = l->tap;
+    geom_setup(l->g, dims, l->tap);
     *out = l.release();
     clear_error();
     return HW_OK;

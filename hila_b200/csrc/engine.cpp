@@ -10,21 +10,27 @@
 
 namespace hw {
 
-int ensure_low_links(const hw_gauge *G, int low) {
+int ensure_low_links(const hw_gauge *G, int low, bool full18) {
     hw_lattice *lat = G->lat;
     hw_context *ctx = lat->ctx;
     const size_t st = lat->stride;
     int rc;
-    if (low == LOW_F32 && !G->f32.ptr) {
+    if (full18) {
+        if (!G->f32a.ptr) {
+            if ((rc = G->f32a.alloc(32 * st * sizeof(float4))) != HW_OK) return rc;
+            if ((rc = G->f32b.alloc(8 * st * sizeof(float2))) != HW_OK) return rc;
+            eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, nullptr, nullptr, nullptr,
+                              G->f32a.as<float4>(), G->f32b.as<float2>(), ctx->stream);
+        }
+    } else if (low == LOW_F32 && !G->f32.ptr) {
         if ((rc = G->f32.alloc(24 * st * sizeof(float4))) != HW_OK) return rc;
         eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, G->f32.as<float4>(), nullptr,
-                          nullptr, ctx->stream);
-    }
-    if (low == LOW_F16 && !G->f16a.ptr) {
+                          nullptr, nullptr, nullptr, ctx->stream);
+    } else if (low == LOW_F16 && !G->f16a.ptr) {
         if ((rc = G->f16a.alloc(8 * st * sizeof(uint4))) != HW_OK) return rc;
         if ((rc = G->f16b.alloc(8 * st * sizeof(uint2))) != HW_OK) return rc;
         eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, nullptr, G->f16a.as<uint4>(),
-                          G->f16b.as<uint2>(), ctx->stream);
+                          G->f16b.as<uint2>(), nullptr, nullptr, ctx->stream);
     }
     HW_CUDA(cudaGetLastError());
     return HW_OK;
@@ -55,7 +61,10 @@ int Engine::init() {
         host_states_[j].status = ENG_IDLE;
     }
     HW_CUDA(cudaMemcpyAsync(d_states_.ptr, host_states_, sizeof(host_states_), cudaMemcpyHostToDevice, ctx_->stream));
-    grid_ = eng_grid_size(low_);
+    // inner links: the 12-real links of the inner precision by default (fewest bytes,
+    // measured fastest); HW_ENGINE_LINKS=18 selects 18-real FP32 links (no third-row rebuild)
+    if (const char *env = std::getenv("HW_ENGINE_LINKS")) full18_ = std::atoi(env) == 18;
+    grid_ = eng_grid_size(low_, kDefaultVariant, full18_ ? 1 : 0, 1);
     // HW_USE_GRAPH=0 runs the iterations from a host loop instead of the captured
     // WHILE graph (profilers see the individual kernel launches)
     if (const char *env = std::getenv("HW_USE_GRAPH")) use_graph_ = std::atoi(env) != 0;
@@ -87,7 +96,7 @@ int Engine::lattice_index(const hw_gauge *G, int *idx) {
         }
     HW_CHECK_ARG(tables_.nlat < kEngMaxLat, "engine holds %d lattices already", kEngMaxLat);
     int rc;
-    if ((rc = ensure_low_links(G, low_)) != HW_OK) return rc;
+    if ((rc = ensure_low_links(G, low_, full18_)) != HW_OK) return rc;
     hw_lattice *lat = G->lat;
     const int l = tables_.nlat;
     EngLattice &L = tables_.lat[l];
@@ -102,6 +111,8 @@ int Engine::lattice_index(const hw_gauge *G, int *idx) {
     L.l32 = G->f32.as<float4>();
     L.l16a = G->f16a.as<uint4>();
     L.l16b = G->f16b.as<uint2>();
+    L.l32a = G->f32a.as<float4>();
+    L.l32b = G->f32b.as<float2>();
     tables_.ntiles += L.ntiles;
     tables_.max_tiles = std::max(tables_.max_tiles, L.ntiles);
     tables_.nlat = l + 1;
@@ -330,8 +341,27 @@ int Engine::build_graph() {
     return HW_OK;
 }
 
+int Engine::configure() {
+    int mask = 0;
+    for (int l = 0; l < tables_.nlat; l++) mask |= tables_.lat[l].l64_planes == 9 ? 1 : 2;
+    if (mask == 0) mask = 1;
+    int variant = kDefaultVariant;
+    if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
+    if (variant < 0 || variant > 3) variant = kDefaultVariant;
+    if (variant != grid_.variant || mask != grid_.planes_mask) {
+        grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
+        if (chunk_exec_) {
+            HW_CUDA(cudaStreamSynchronize(ctx_->stream));
+            cudaGraphExecDestroy(chunk_exec_);
+            chunk_exec_ = nullptr;
+        }
+    }
+    return HW_OK;
+}
+
 int Engine::launch_chunk(int iters) {
     int rc;
+    if ((rc = configure()) != HW_OK) return rc;
     if ((rc = ensure_partials()) != HW_OK) return rc;
     if (use_graph_ && !chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
     if ((rc = upload_tables()) != HW_OK) return rc;

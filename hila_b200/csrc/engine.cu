@@ -6,6 +6,8 @@
 // summed per slot in tile order by the last block to finish the lattice, so a
 // slot's arithmetic does not depend on which other slots share the launch:
 // a solve gives bitwise the same result alone and inside any batch.
+#include <type_traits>
+
 #include "engine.h"
 #include "reduce.cuh"
 #include "storage.cuh"
@@ -35,6 +37,18 @@ struct Low<LOW_F16> {
         return Sp{static_cast<uint4 *>(p), n, stride};
     }
     static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l16a, L.l16b, L.stride}; }
+};
+
+// links of the inner phases: the precision's own 12-real format, or 18-real FP32
+template <int LOW, bool FULL18>
+struct InnerLinks {
+    using Lk = typename Low<LOW>::Lk;
+    static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Low<LOW>::lk(L); }
+};
+template <int LOW>
+struct InnerLinks<LOW, true> {
+    using Lk = LinksF32x18;
+    static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l32a, L.l32b, L.stride}; }
 };
 
 __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
@@ -110,43 +124,58 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
     }
 }
 
-// FP64 reliable-update phases R2..R5.  acc = (H in)(i) in FP64.
+// FP64 reliable-update phases R2..R5.  acc = (H in)(i) in FP64.  The problem's
+// pointers are copied to locals first: stores through them could otherwise alias
+// the table and force reloads.
 template <int PHASE, int LOW>
 __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i, Spinor<double> &acc,
                                         double *red) {
     const double k2 = pr.kappa * pr.kappa;
+    const bool solve = pr.mode == ENG_MODE_SOLVE;
     if (PHASE == PH_R2 || PHASE == PH_R4) {
         SpinorF64{pr.t64, stride}.store(i, acc);
     } else if (PHASE == PH_R3) {
+        const double2 *__restrict__ x = pr.x;
+        const double2 *__restrict__ b = pr.b;
+        double2 *__restrict__ sp = pr.s;
         double n2 = 0, d2 = 0;
+        if (solve) {
 #pragma unroll
-        for (int c = 0; c < 12; c++) {
-            Cx<double> mx = ldc(pr.x, stride, c, i) - k2 * acc.s[c / 3][c % 3];
-            if (pr.mode == ENG_MODE_SOLVE) {
-                Cx<double> bv = ldc(pr.b, stride, c, i);
-                Cx<double> sv = bv - mx;
-                stc(pr.s, stride, c, i, sv);
+            for (int c = 0; c < 12; c++) {
+                const Cx<double> mx = ldc(x, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+                const Cx<double> bv = ldc(b, stride, c, i);
+                const Cx<double> sv = bv - mx;
+                stc(sp, stride, c, i, sv);
                 n2 += norm2(sv);
                 d2 += norm2(bv);
-            } else {
-                stc(pr.s, stride, c, i, mx);
             }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 12; c++) stc(sp, stride, c, i, ldc(x, stride, c, i) - k2 * acc.s[c / 3][c % 3]);
         }
         red[0] = n2;
         red[1] = d2;
     } else if (PHASE == PH_R5) {
+        const double2 *__restrict__ sv = pr.s;
+        const double2 *__restrict__ b = pr.b;
         double n2 = 0, d2 = 0;
         Spinor<float> rl;
+        if (solve) {
 #pragma unroll
-        for (int c = 0; c < 12; c++) {
-            Cx<double> v = ldc(pr.s, stride, c, i) - k2 * acc.s[c / 3][c % 3];
-            if (pr.mode == ENG_MODE_NORMAL) {
-                Cx<double> bv = ldc(pr.b, stride, c, i);
-                v = bv - v;
-                d2 += norm2(bv);
+            for (int c = 0; c < 12; c++) {
+                const Cx<double> v = ldc(sv, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+                n2 += norm2(v);
+                rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};
             }
-            n2 += norm2(v);
-            rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};
+        } else {
+#pragma unroll
+            for (int c = 0; c < 12; c++) {
+                const Cx<double> bv = ldc(b, stride, c, i);
+                const Cx<double> v = bv - (ldc(sv, stride, c, i) - k2 * acc.s[c / 3][c % 3]);
+                d2 += norm2(bv);
+                n2 += norm2(v);
+                rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};
+            }
         }
         Low<LOW>::sp(pr.r, pr.rn, stride).store(i, rl);
         red[0] = n2;
@@ -223,16 +252,54 @@ __device__ void finish(EngState &s, const EngProblem &pr, const double *tot, int
 
 // ------------------------------------------------------------------ hop phases
 
-template <int PHASE, int LOW>
-__global__ void __launch_bounds__(kEngTile) k_eng_hop(EngPtrs P) {
-    constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2 || PHASE == PH_R2 || PHASE == PH_R3) ? 1 : -1;
-    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R2 || PHASE == PH_R4) ? 1 : 0;
-    constexpr bool F64 = PHASE >= PH_R2 && PHASE <= PH_R5;
-    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4) ? 1 : ((PHASE == PH_R3 || PHASE == PH_R5) ? 2 : 0);
+// Arrival of one tile of lattice l; the last tile of the lattice sums every
+// active slot's partials in tile order and runs the finisher.
+template <int PHASE, int NRED>
+__device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLattice &La, int l, double *smem,
+                                                  bool &last) {
+    const EngTables *T = P.T;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned t = atomicAdd(P.tickets + l, 1u);
+        last = (t == (unsigned)La.ntiles - 1u);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        const int nt = La.ntiles;
+        const int max_tiles = T->max_tiles;
+        for (int q = 0; q < La.nprob; q++) {
+            const int j = La.prob[q];
+            if (!active<PHASE>(P.S[j])) continue;
+            double tot[2] = {0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < NRED; k++) {
+                const double *pp = P.partials + ((size_t)j * 2 + k) * max_tiles;
+                double s = 0.0;
+                for (int t2 = threadIdx.x; t2 < nt; t2 += kEngTile) s += __ldcg(pp + t2);
+                tot[k] = block_sum<kEngTile>(s, smem);
+            }
+            if (threadIdx.x == 0) finish<PHASE>(P.S[j], T->prob[j], tot, P.ctl);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) P.tickets[l] = 0u;
+    }
+    __syncthreads();
+}
+
+// Inner phases P1..P4 in low precision.  Each thread owns one site and up to
+// NR right-hand sides at a time, so links, their third rows and the neighbour
+// indices are shared by the NR solves.
+template <int PHASE, int LOW, int NR, int MINB, bool FULL18>
+__global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
+    constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2) ? 1 : -1;
+    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3) ? 1 : 0;
+    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4) ? 1 : 0;
     using L = Low<LOW>;
     __shared__ double smem[kEngTile / 32];
     __shared__ bool last;
-    if (PHASE >= PH_R1 && PHASE <= PH_R5 && *(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
+    __shared__ int s_act[kEngMaxRhs];
+    __shared__ int s_na;
     const EngTables *T = P.T;
     const int ntiles = T->ntiles;
     const int max_tiles = T->max_tiles;
@@ -244,67 +311,124 @@ __global__ void __launch_bounds__(kEngTile) k_eng_hop(EngPtrs P) {
         const int lt = tile - La.tile0;
         const int i = lt * kEngTile + threadIdx.x;
         const bool valid = i < g.Vh;
-        const int nprob = La.nprob;
-        for (int q = 0; q < nprob; q++) {
-            const int j = La.prob[q];
-            if (!active<PHASE>(P.S[j])) continue;
-            const EngProblem &pr = T->prob[j];
-            double red[2] = {0.0, 0.0};
-            if (valid) {
-                if constexpr (F64) {
-                    const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
-                    Spinor<double> acc;
-                    if (La.l64_planes == 9)
-                        hop_site<SIGN>(g, OUTPAR, i, SpinorF64{const_cast<double2 *>(in), stride},
-                                       LinksF64x18{La.l64, stride}, acc);
-                    else
-                        hop_site<SIGN>(g, OUTPAR, i, SpinorF64{const_cast<double2 *>(in), stride},
-                                       LinksF64x12{La.l64, stride}, acc);
-                    epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
-                } else {
-                    void *in = (PHASE == PH_P1) ? pr.p : (PHASE == PH_P3 ? pr.Dp : pr.t);
-                    float *inn = (PHASE == PH_P1) ? pr.pn : (PHASE == PH_P3 ? pr.Dpn : pr.tn);
-                    Spinor<float> acc;
-                    hop_site<SIGN>(g, OUTPAR, i, L::sp(in, inn, stride), L::lk(La), acc);
-                    epi_low<PHASE, LOW>(pr, P.S[j], stride, i, acc, red);
-                }
+        if (threadIdx.x == 0) {
+            int na = 0;
+            for (int q = 0; q < La.nprob; q++) {
+                const int j = La.prob[q];
+                if (active<PHASE>(P.S[j])) s_act[na++] = j;
             }
-            if constexpr (NRED > 0) {
+            s_na = na;
+        }
+        __syncthreads();
+        const int na = s_na;
+        SiteNbrs nb;
+        if (valid && na > 0) nb = site_neighbours(g, i, OUTPAR);
+        for (int g0 = 0; g0 < na; g0 += NR) {
+            const int cnt = min(NR, na - g0);
+            typename L::Sp in[NR];
 #pragma unroll
-                for (int k = 0; k < NRED; k++) {
-                    double s = block_sum<kEngTile>(red[k], smem);
-                    if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = s;
+            for (int r = 0; r < NR; r++) {
+                const EngProblem &pr = T->prob[s_act[g0 + min(r, cnt - 1)]];
+                void *ip = (PHASE == PH_P1) ? pr.p : (PHASE == PH_P3 ? pr.Dp : pr.t);
+                float *inn = (PHASE == PH_P1) ? pr.pn : (PHASE == PH_P3 ? pr.Dpn : pr.tn);
+                in[r] = L::sp(ip, inn, stride);
+            }
+            Spinor<float> acc[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+#pragma unroll
+                for (int c = 0; c < 12; c++) acc[r].s[c / 3][c % 3] = {0.f, 0.f};
+            if (valid) {
+                const typename InnerLinks<LOW, FULL18>::Lk U = InnerLinks<LOW, FULL18>::lk(La);
+                hop_dir_multi<0, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                hop_dir_multi<1, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                hop_dir_multi<2, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                hop_dir_multi<3, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+            }
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                if (r < cnt) {
+                    const int j = s_act[g0 + r];
+                    double red[2] = {0.0, 0.0};
+                    if (valid) epi_low<PHASE, LOW>(T->prob[j], P.S[j], stride, i, acc[r], red);
+                    if constexpr (NRED > 0) {
+                        double sum = block_sum<kEngTile>(red[0], smem);
+                        if (threadIdx.x == 0) P.partials[((size_t)j * 2) * max_tiles + lt] = sum;
+                    }
                 }
             }
         }
-        if constexpr (NRED > 0) {
-            if (threadIdx.x == 0) {
-                __threadfence();
-                unsigned t = atomicAdd(P.tickets + l, 1u);
-                last = (t == (unsigned)La.ntiles - 1u);
+        __syncthreads();  // s_act is rewritten by the next tile
+        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED>(P, La, l, smem, last);
+    }
+}
+
+// FP64 reliable-update phases R2..R5 for lattices whose FP64 links have PLANES
+// planes per (parity, dir); a second launch serves the other format if present.
+template <int PHASE, int LOW, int PLANES>
+__global__ void __launch_bounds__(kEngTile, 2) k_eng_f64(EngPtrs P) {
+    constexpr int SIGN = (PHASE == PH_R2 || PHASE == PH_R3) ? 1 : -1;
+    constexpr int OUTPAR = (PHASE == PH_R2 || PHASE == PH_R4) ? 1 : 0;
+    constexpr int NRED = (PHASE == PH_R3 || PHASE == PH_R5) ? 2 : 0;
+    using Lk = typename std::conditional<PLANES == 9, LinksF64x18, LinksF64x12>::type;
+    __shared__ double smem[kEngTile / 32];
+    __shared__ bool last;
+    __shared__ int s_act[kEngMaxRhs];
+    __shared__ int s_na;
+    if (*(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
+    const EngTables *T = P.T;
+    const int ntiles = T->ntiles;
+    const int max_tiles = T->max_tiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int l = find_lattice(T, tile);
+        const EngLattice &La = T->lat[l];
+        if (La.l64_planes != PLANES) continue;
+        if (threadIdx.x == 0) {
+            int na = 0;
+            for (int q = 0; q < La.nprob; q++) {
+                const int j = La.prob[q];
+                if (active<PHASE>(P.S[j])) s_act[na++] = j;
             }
-            __syncthreads();
-            if (last) {
-                __threadfence();
-                const int nt = La.ntiles;
-                for (int q = 0; q < nprob; q++) {
-                    const int j = La.prob[q];
-                    if (!active<PHASE>(P.S[j])) continue;
-                    double tot[2] = {0.0, 0.0};
+            s_na = na;
+        }
+        __syncthreads();
+        const int na = s_na;
+        if (na > 0) {
+            const Geom g = La.g;
+            const int stride = La.stride;
+            const int lt = tile - La.tile0;
+            const int i = lt * kEngTile + threadIdx.x;
+            const bool valid = i < g.Vh;
+            SiteNbrs nb;
+            if (valid) nb = site_neighbours(g, i, OUTPAR);
+            const Lk U{La.l64, stride};
+            for (int a = 0; a < na; a++) {
+                const int j = s_act[a];
+                const EngProblem &pr = T->prob[j];
+                double red[2] = {0.0, 0.0};
+                if (valid) {
+                    const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
+                    const SpinorF64 sin[1] = {SpinorF64{const_cast<double2 *>(in), stride}};
+                    Spinor<double> acc[1];
+#pragma unroll
+                    for (int c = 0; c < 12; c++) acc[0].s[c / 3][c % 3] = {0.0, 0.0};
+                    hop_dir_multi<0, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
+                    hop_dir_multi<1, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
+                    hop_dir_multi<2, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
+                    hop_dir_multi<3, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
+                    epi_f64<PHASE, LOW>(pr, stride, i, acc[0], red);
+                }
+                if constexpr (NRED > 0) {
 #pragma unroll
                     for (int k = 0; k < NRED; k++) {
-                        const double *pp = P.partials + ((size_t)j * 2 + k) * max_tiles;
-                        double s = 0.0;
-                        for (int t2 = threadIdx.x; t2 < nt; t2 += kEngTile) s += __ldcg(pp + t2);
-                        tot[k] = block_sum<kEngTile>(s, smem);
+                        double sum = block_sum<kEngTile>(red[k], smem);
+                        if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
                     }
-                    if (threadIdx.x == 0) finish<PHASE>(P.S[j], T->prob[j], tot, P.ctl);
-                    __syncthreads();
                 }
-                if (threadIdx.x == 0) P.tickets[l] = 0u;
             }
-            __syncthreads();
         }
+        __syncthreads();  // s_act is rewritten by the next tile
+        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED>(P, La, l, smem, last);
     }
 }
 
@@ -387,10 +511,29 @@ __global__ void k_eng_chunk_begin(EngPtrs P) { P.ctl[0] = 0; }
 
 // FP64 link planes (first six elements = rows 0 and 1) -> FP32 / FP16 12-real planes
 __global__ void k_eng_links(Geom g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                            uint2 *l16b) {
+                            uint2 *l16b, float4 *l32a, float2 *l32b) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int pd = blockIdx.y;  // parity*4 + dir
     if (i >= g.Vh) return;
+    if (l32a) {
+        // all 18 reals; a 12-real FP64 source gets its third row rebuilt in FP64 first
+        Su3<double> u;
+        for (int k = 0; k < 9; k++) {
+            if (k < planes) {
+                double2 v = l64[((size_t)pd * planes + k) * stride + i];
+                u.e[k / 3][k % 3] = {v.x, v.y};
+            }
+        }
+        if (planes == 6) reconstruct_row2(u);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int e0 = 2 * k, e1 = 2 * k + 1;
+            l32a[((size_t)pd * 4 + k) * stride + i] =
+                make_float4((float)u.e[e0 / 3][e0 % 3].re, (float)u.e[e0 / 3][e0 % 3].im,
+                            (float)u.e[e1 / 3][e1 % 3].re, (float)u.e[e1 / 3][e1 % 3].im);
+        }
+        l32b[(size_t)pd * stride + i] = make_float2((float)u.e[2][2].re, (float)u.e[2][2].im);
+    }
     float e[12];
 #pragma unroll
     for (int k = 0; k < 6; k++) {
@@ -417,27 +560,65 @@ __global__ void k_eng_links(Geom g, const double2 *l64, int planes, int stride, 
     }
 }
 
+template <int PHASE, int LOW>
+void launch_f64(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    if (G.planes_mask & 1) k_eng_f64<PHASE, LOW, 9><<<G.f64, kEngTile, 0, s>>>(P);
+    if (G.planes_mask & 2) k_eng_f64<PHASE, LOW, 6><<<G.f64, kEngTile, 0, s>>>(P);
+}
+
+template <int LOW, int NR, int MINB, bool FULL18>
+void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    k_eng_low<PH_P1, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P2, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P3, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P4, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_vec<PH_R1, LOW><<<G.low, kEngTile, 0, s>>>(P);
+    launch_f64<PH_R2, LOW>(P, G, s);
+    launch_f64<PH_R3, LOW>(P, G, s);
+    launch_f64<PH_R4, LOW>(P, G, s);
+    launch_f64<PH_R5, LOW>(P, G, s);
+    k_eng_vec<PH_P5, LOW><<<G.low, kEngTile, 0, s>>>(P);
+}
+
+// Launch shapes of the low-precision phases (EngGrid::variant):
+//   0: one right-hand side per thread, <= 128 registers (4 blocks of 128 per SM)
+//   1: one right-hand side per thread, <= 102 registers (5 blocks)
+//   2: one right-hand side per thread, <= 85 registers (6 blocks)
+//   3: two right-hand sides per thread sharing the links, <= 128 registers
+// each with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
+template <int LOW, bool FULL18>
+void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    switch (G.variant) {
+    case 1:
+        enqueue_iteration_t<LOW, 1, 5, FULL18>(P, G, s);
+        break;
+    case 2:
+        enqueue_iteration_t<LOW, 1, 6, FULL18>(P, G, s);
+        break;
+    case 3:
+        enqueue_iteration_t<LOW, 2, 4, FULL18>(P, G, s);
+        break;
+    default:
+        enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s);
+        break;
+    }
+}
+
 template <int LOW>
-void enqueue_iteration_t(const EngPtrs &P, int grid, int grid64, cudaStream_t s) {
-    k_eng_hop<PH_P1, LOW><<<grid, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_P2, LOW><<<grid, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_P3, LOW><<<grid, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_P4, LOW><<<grid, kEngTile, 0, s>>>(P);
-    k_eng_vec<PH_R1, LOW><<<grid, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_R2, LOW><<<grid64, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_R3, LOW><<<grid64, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_R4, LOW><<<grid64, kEngTile, 0, s>>>(P);
-    k_eng_hop<PH_R5, LOW><<<grid64, kEngTile, 0, s>>>(P);
-    k_eng_vec<PH_P5, LOW><<<grid, kEngTile, 0, s>>>(P);
+void enqueue_iteration_nr(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    if (G.full18)
+        enqueue_iteration_v<LOW, true>(P, G, s);
+    else
+        enqueue_iteration_v<LOW, false>(P, G, s);
 }
 
 }  // namespace
 
 void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
     if (low == LOW_F16)
-        enqueue_iteration_t<LOW_F16>(P, G.low, G.f64, s);
+        enqueue_iteration_nr<LOW_F16>(P, G, s);
     else
-        enqueue_iteration_t<LOW_F32>(P, G.low, G.f64, s);
+        enqueue_iteration_nr<LOW_F32>(P, G, s);
 }
 
 void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
@@ -448,23 +629,44 @@ void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphCondit
 void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s) { k_eng_chunk_begin<<<1, 1, 0, s>>>(P); }
 
 void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                       uint2 *l16b, cudaStream_t s) {
+                       uint2 *l16b, float4 *l32a, float2 *l32b, cudaStream_t s) {
     dim3 grid((g.Vh + 255) / 256, 8);
-    k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b);
+    k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b, l32a, l32b);
 }
 
-EngGrid eng_grid_size(int low) {
-    int dev = 0, sms = 148, lo = 0, hi = 0;
+template <int LOW, int NR, int MINB>
+int occupancy_low() {
+    int lo = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_low<PH_P4, LOW, NR, MINB, true>, kEngTile, 0);
+    return lo < 1 ? 1 : lo;
+}
+
+template <int LOW>
+int occupancy_variant(int v) {
+    switch (v) {
+    case 1:
+        return occupancy_low<LOW, 1, 5>();
+    case 2:
+        return occupancy_low<LOW, 1, 6>();
+    case 3:
+        return occupancy_low<LOW, 2, 4>();
+    default:
+        return occupancy_low<LOW, 1, 4>();
+    }
+}
+
+EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask) {
+    int dev = 0, sms = 148, lo = 1, hi = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (low == LOW_F16)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_hop<PH_P4, LOW_F16>, kEngTile, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_hop<PH_P4, LOW_F32>, kEngTile, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hi, k_eng_hop<PH_R5, LOW_F32>, kEngTile, 0);
+    lo = low == LOW_F16 ? occupancy_variant<LOW_F16>(variant) : occupancy_variant<LOW_F32>(variant);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hi, k_eng_f64<PH_R5, LOW_F32, 9>, kEngTile, 0);
     EngGrid G;
-    G.low = sms * (lo < 1 ? 1 : lo);
+    G.low = sms * lo;
     G.f64 = sms * (hi < 1 ? 1 : hi);
+    G.variant = variant;
+    G.full18 = full18;
+    G.planes_mask = planes_mask;
     return G;
 }
 

@@ -52,6 +52,8 @@ struct EngLattice {
     const float4 *l32;   // FP32, 12 reals: 3 float4 planes per (parity, dir)
     const uint4 *l16a;   // FP16, 12 reals: 8 halves ...
     const uint2 *l16b;   // ... + 4 halves per link
+    const float4 *l32a;  // FP32, 18 reals: 4 float4 planes ...
+    const float2 *l32b;  // ... + 1 float2 plane per (parity, dir)
 };
 
 struct EngProblem {
@@ -109,6 +111,9 @@ struct EngPtrs {
 struct EngGrid {
     int low;  // blocks of the low-precision phases (all SMs x resident blocks)
     int f64;  // blocks of the FP64 reliable-update phases
+    int variant;  // launch shape of the low-precision phases (engine.cu)
+    int full18;   // 1: inner phases read 18-real FP32 links; 0: the 12-real links of the precision
+    int planes_mask;  // FP64 link formats present: bit 0 = 18 reals, bit 1 = 12 reals
 };
 
 enum EngPhase : int { PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R5, PH_P5 };
@@ -124,8 +129,8 @@ void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphCondit
 void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s);
 // Convert FP64 link planes to the 12-real FP32 / FP16 planes of the inner solve.
 void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                       uint2 *l16b, cudaStream_t s);
-// grid sizes (blocks) of the engine kernels on the current device
-EngGrid eng_grid_size(int low);
+                       uint2 *l16b, float4 *l32a, float2 *l32b, cudaStream_t s);
+// launch configuration of the engine kernels on the current device
+EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask);
 
 }  // namespace hw

@@ -58,6 +58,7 @@ class Engine {
     int ensure_slot_buffers(int slot, int stride);
     int build_graph();
     void set_ptrs();
+    int configure();
     int ensure_partials();
 
     hw_context *ctx_;
@@ -76,11 +77,14 @@ class Engine {
     cudaGraphExec_t chunk_exec_ = nullptr;
     bool tables_dirty_ = true;
     bool use_graph_ = true;
+    bool full18_ = false;
+    // launch shape of the inner phases (engine.cu): one RHS per thread, 6 blocks per SM
+    static constexpr int kDefaultVariant = 2;
 };
 
 // per-context engine for a low precision (LOW_F32 / LOW_F16), created on first use
 int get_engine(hw_context *ctx, int low, Engine **eng);
 // make the FP32 / FP16 link copies of a gauge field
-int ensure_low_links(const hw_gauge *G, int low);
+int ensure_low_links(const hw_gauge *G, int low, bool full18);
 
 }  // namespace hw

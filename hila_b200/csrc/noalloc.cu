@@ -89,14 +89,7 @@ extern "C" int hw_wilson_evenodd_apply_noalloc(const int dims[4], int t_antiperi
     if (rc != HW_OK) return rc;
 
     Geom g{};
-    for (int d = 0; d < 4; d++) g.L[d] = dims[d];
-    g.lxh = dims[0] / 2;
-    g.Vh = (int)Vh;
-    g.sy = g.lxh;
-    g.sz = g.lxh * dims[1];
-    g.st = g.lxh * dims[1] * dims[2];
-    g.tap = t_antiperiodic ? 1 : 0;
-    g.hop_variant = 0;
+    geom_setup(g, dims, t_antiperiodic);
     const GaugeF64 U{reinterpret_cast<const double2 *>(links), stride, link_format == 12 ? 6 : 9};
     const HalfF64 in{const_cast<double2 *>(reinterpret_cast<const double2 *>(in_even)), stride};
     const HalfF64 out{reinterpret_cast<double2 *>(out_even), stride};

@@ -45,6 +45,10 @@ struct SpinorF64 {
             w.s[c / 3][c % 3] = {v.x, v.y};
         }
     }
+    __device__ __forceinline__ void load_raw(int i, Spinor<double> &w, double &sc) const {
+        sc = 1.0;
+        load(i, w);
+    }
     __device__ __forceinline__ void store(int i, const Spinor<double> &w) const {
 #pragma unroll
         for (int c = 0; c < 12; c++) p[(size_t)c * stride + i] = make_double2(w.s[c / 3][c % 3].re, w.s[c / 3][c % 3].im);
@@ -65,6 +69,10 @@ struct SpinorF32 {
         }
     }
     __device__ __forceinline__ void load_cached(int i, Spinor<float> &w) const { load(i, w); }
+    __device__ __forceinline__ void load_raw(int i, Spinor<float> &w, float &sc) const {
+        sc = 1.0f;
+        load(i, w);
+    }
     __device__ __forceinline__ void store(int i, const Spinor<float> &w) const {
 #pragma unroll
         for (int k = 0; k < 6; k++) {
@@ -98,6 +106,21 @@ struct SpinorF16 {
         }
     }
     __device__ __forceinline__ void load_cached(int i, Spinor<float> &w) const { load(i, w); }
+    // unscaled values; the caller multiplies by *sc (the site norm)
+    __device__ __forceinline__ void load_raw(int i, Spinor<float> &w, float &sc) const {
+        sc = __ldg(norm + i);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v = __ldg(p + (size_t)k * stride + i);
+            const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float2 f = __half22float2(h[q]);
+                int c = 4 * k + q;
+                w.s[c / 3][c % 3] = {f.x, f.y};
+            }
+        }
+    }
     __device__ __forceinline__ void store(int i, const Spinor<float> &w) const {
         float m = 0.f;
 #pragma unroll
@@ -166,6 +189,28 @@ struct LinksF32x12 {
             u.e[e1 / 3][e1 % 3] = {v.z, v.w};
         }
         reconstruct_row2(u);
+    }
+};
+
+// FP32, all 18 reals: 4 float4 planes (elements 0..7) + 1 float2 plane (element 8)
+// per (parity, dir).  No third-row rebuild: used where the same links serve many
+// right-hand sides from cache and instructions, not bytes, bound the kernel.
+struct LinksF32x18 {
+    using R = float;
+    const float4 *a;
+    const float2 *b;
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
+        const float4 *pa = a + (size_t)((par * 4 + dir) * 4) * stride + i;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float4 v = __ldg(pa + (size_t)k * stride);
+            int e0 = 2 * k, e1 = 2 * k + 1;
+            u.e[e0 / 3][e0 % 3] = {v.x, v.y};
+            u.e[e1 / 3][e1 % 3] = {v.z, v.w};
+        }
+        float2 w = __ldg(b + (size_t)(par * 4 + dir) * stride + i);
+        u.e[2][2] = {w.x, w.y};
     }
 };
 
@@ -239,6 +284,44 @@ __device__ __forceinline__ void hop_dir(const SiteNbrs &n, int par, int i, const
         su3_adj_mul(u, h0, v0);
         su3_adj_mul(u, h1, v1);
         expand_add<MU, -SIGN>(acc, v0, v1);
+    }
+}
+
+// Hopping term for NR right-hand sides that share the links: every link is
+// loaded (and its third row rebuilt) once for all of them.  in[r] is read at
+// the neighbour sites; cnt <= NR of them are live.
+template <int MU, int SIGN, int NR, class SpIn, class Lk, typename R>
+__device__ __forceinline__ void hop_dir_multi(const SiteNbrs &n, int par, int i, const SpIn (&in)[NR], int cnt,
+                                              const Lk &U, Spinor<R> (&acc)[NR]) {
+    Cx<R> h0[3], h1[3], v0[3], v1[3];
+    Su3<R> u;
+    U.load(par, MU, i, u);
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r < cnt) {
+            Spinor<R> w;
+            R sc;
+            in[r].load_raw(n.fwd[MU], w, sc);
+            if (MU == 3 && n.tfwd_wrap) sc = -sc;
+            project<MU, SIGN>(w, h0, h1);
+            su3_mul(u, h0, v0);
+            su3_mul(u, h1, v1);
+            expand_add_scaled<MU, SIGN>(acc[r], v0, v1, sc);
+        }
+    }
+    U.load(1 - par, MU, n.bwd[MU], u);
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r < cnt) {
+            Spinor<R> w;
+            R sc;
+            in[r].load_raw(n.bwd[MU], w, sc);
+            if (MU == 3 && n.tbwd_wrap) sc = -sc;
+            project<MU, -SIGN>(w, h0, h1);
+            su3_adj_mul(u, h0, v0);
+            su3_adj_mul(u, h1, v1);
+            expand_add_scaled<MU, -SIGN>(acc[r], v0, v1, sc);
+        }
     }
 }
 

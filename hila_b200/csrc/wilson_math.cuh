@@ -213,12 +213,63 @@ __device__ __forceinline__ void expand_add(Spinor<R> &acc, const Cx<R> h0[3], co
     }
 }
 
+// a + s v and a + s (i v), component-wise FMAs
+template <typename R>
+__device__ __forceinline__ Cx<R> axpy(Cx<R> a, R s, Cx<R> v) {
+    return {fma(s, v.re, a.re), fma(s, v.im, a.im)};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> axpy_i(Cx<R> a, R s, Cx<R> v) {
+    return {fma(-s, v.im, a.re), fma(s, v.re, a.im)};
+}
+
+// acc += sc * E_{dir,sign}(h): expand_add with a scale folded into the FMAs
+// (the per-site norm of FP16 storage and the antiperiodic sign cost nothing).
+template <int DIR, int SIGN, typename R>
+__device__ __forceinline__ void expand_add_scaled(Spinor<R> &acc, const Cx<R> h0[3], const Cx<R> h1[3], R sc) {
+    const R sp = SIGN > 0 ? sc : -sc;  // sign * sc
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        acc.s[0][k] = axpy(acc.s[0][k], sc, h0[k]);
+        acc.s[1][k] = axpy(acc.s[1][k], sc, h1[k]);
+        if (DIR == 0) {  // r2 = -s i h1, r3 = -s i h0
+            acc.s[2][k] = axpy_i(acc.s[2][k], -sp, h1[k]);
+            acc.s[3][k] = axpy_i(acc.s[3][k], -sp, h0[k]);
+        } else if (DIR == 1) {  // r2 = s h1, r3 = -s h0
+            acc.s[2][k] = axpy(acc.s[2][k], sp, h1[k]);
+            acc.s[3][k] = axpy(acc.s[3][k], -sp, h0[k]);
+        } else if (DIR == 2) {  // r2 = -s i h0, r3 = s i h1
+            acc.s[2][k] = axpy_i(acc.s[2][k], -sp, h0[k]);
+            acc.s[3][k] = axpy_i(acc.s[3][k], sp, h1[k]);
+        } else {  // r2 = s h0, r3 = s h1
+            acc.s[2][k] = axpy(acc.s[2][k], sp, h0[k]);
+            acc.s[3][k] = axpy(acc.s[3][k], sp, h1[k]);
+        }
+    }
+}
+
 // ----------------------------------------------------------------- geometry
 //
 // Even-odd layout: a site with lexicographic index
 // lex = x + Lx*(y + Ly*(z + Lz*t)) and parity (x+y+z+t)&1 lives at
 // checkerboard index lex/2 inside the half-lattice array of its parity
 // (lattice.cpp:171-184 with even sites first).  Lx must be even.
+
+// Exact unsigned division by a divisor fixed at set-up: q = umulhi64(n, m) with
+// m = ceil(2^64 / d) equals floor(n / d) for all n, d < 2^32 (the rounding error
+// n * (m d - 2^64) / 2^64 < n d / 2^64 < 1 cannot reach the next multiple).
+// m = 0 encodes d = 1.
+struct FastDiv {
+    unsigned long long m;
+    unsigned d;
+    __host__ __device__ void init(unsigned div) {
+        d = div;
+        m = (div <= 1) ? 0ull : (~0ull / div) + 1ull;
+    }
+    __device__ __forceinline__ unsigned div(unsigned n) const {
+        return m ? (unsigned)__umul64hi((unsigned long long)n, m) : n;
+    }
+};
 
 struct Geom {
     int L[4];       // Lx, Ly, Lz, Lt
@@ -227,7 +278,23 @@ struct Geom {
     int sy, sz, st; // checkerboard strides of y, z, t: lxh, lxh*Ly, lxh*Ly*Lz
     int tap;        // 1: fermion values crossing the t boundary are negated
     int hop_variant;  // launch shape of the FP64 hop kernels (host-side choice, see dslash_f64.cu)
+    FastDiv dx, dy, dz;  // division by lxh, Ly, Lz
 };
+
+// fill a Geom for dims (all even) and the fermion boundary condition in t
+inline void geom_setup(Geom &g, const int dims[4], int tap) {
+    for (int d = 0; d < 4; d++) g.L[d] = dims[d];
+    g.lxh = dims[0] / 2;
+    g.Vh = (int)((long)dims[0] * dims[1] * dims[2] * dims[3] / 2);
+    g.sy = g.lxh;
+    g.sz = g.lxh * dims[1];
+    g.st = g.lxh * dims[1] * dims[2];
+    g.tap = tap ? 1 : 0;
+    g.hop_variant = 0;
+    g.dx.init((unsigned)g.lxh);
+    g.dy.init((unsigned)dims[1]);
+    g.dz.init((unsigned)dims[2]);
+}
 
 struct SiteNbrs {
     int fwd[4], bwd[4];  // checkerboard index of x+mu, x-mu (opposite parity)
@@ -237,13 +304,13 @@ struct SiteNbrs {
 // neighbours of checkerboard site i of parity par
 __device__ __forceinline__ SiteNbrs site_neighbours(const Geom &g, int i, int par) {
     SiteNbrs n;
-    int xh = i % g.lxh;
-    int r = i / g.lxh;
-    int y = r % g.L[1];
-    r /= g.L[1];
-    int z = r % g.L[2];
-    int t = r / g.L[2];
-    int x = 2 * xh + ((y + z + t + par) & 1);
+    const int q1 = (int)g.dx.div((unsigned)i);
+    const int xh = i - q1 * g.lxh;
+    const int q2 = (int)g.dy.div((unsigned)q1);
+    const int y = q1 - q2 * g.L[1];
+    const int t = (int)g.dz.div((unsigned)q2);
+    const int z = q2 - t * g.L[2];
+    const int x = 2 * xh + ((y + z + t + par) & 1);
     int base = i - xh;
     int xp = (x + 1 == g.L[0]) ? 0 : x + 1;
     int xm = (x == 0) ? g.L[0] - 1 : x - 1;
