@@ -5,15 +5,21 @@
 
 Workloads (seeded synthetic inputs with the shapes of the reference's
 benchmark configurations; no external data):
-  cg      (default) 32^4, links exp(i 0.3 H), kappa = 0.124, Gaussian source;
+  cg      32^4, links exp(i 0.3 H), kappa = 0.124, Gaussian source;
           one step = one solve of M x = b to true residual |b - M x|/|b| <= 1e-10.
           metric: CG solves/s.
   dslash  32^4, the even-odd operator applied with its dagger; one step =
           100 x (apply + dagger).  metric: dslash HBM GB/s (algorithmic bytes).
-  mrhs    the cg workload with 12 Gaussian sources per step solved together by the
-          batched mixed-precision engine (FP16 inner solve by default).
-          metric: CG solves/s.
+  mrhs    (default) the cg workload with 12 Gaussian sources per step solved together
+          by the batched mixed-precision engine (FP16 inner solve, FP64 reliable
+          updates), next to the plain FP64 CG on the same workload in the same run.
+          metric: CG solves/s (mixed), with fp64_solves_per_s and the speed-up.
   cg8     8^4, kappa = 0.12, plain FP64 CG (the CPU-runnable configuration).
+  serve   Poisson stream of solve requests (default 200 at 6 requests/s; --requests,
+          --rate) over 8 device-resident gauge fields 8^4 .. 32^4, each request with
+          1..12 sources, kappa in [0.115, 0.124], accuracy 1e-10, through the
+          continuous-batching server; the same request sequence is also served by the
+          plain FP64 CG one source at a time (FIFO).  metric: solves/s, p50/p99 latency.
 
 Multi-GPU runs (torchrun) are replicas: every rank solves its own copy of the
 workload; value = total solves over all ranks / max-over-ranks device time.
@@ -44,6 +50,10 @@ WORKLOADS = {
     "mrhs": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101, nrhs=12),
     "cg8": dict(dims=(8, 8, 8, 8), eps=0.3, kappa=0.12, tol=1e-10, link_seed=1, src_seed=2),
     "dslash": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=None, link_seed=100, src_seed=101),
+    "serve": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101,
+                  lattices=[(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (20, 20, 20, 20),
+                            (24, 24, 24, 24), (28, 28, 28, 28), (32, 32, 32, 32)],
+                  requests=200, rate=6.0, kappa_range=(0.115, 0.124), nrhs_range=(1, 12)),
 }
 # CG iterations of one solve of each workload (FP64 CG on M^dag M, true residual 1e-10), used to turn the
 # reference arm's per-iteration time into solves/s.  Measured by the FP64 GPU CG on exactly these seeded
@@ -308,6 +318,22 @@ def run_ours(args, dist: Dist):
                "d2h_bytes_per_step": int(nrhs * pouts[0].array.nbytes)}
         for pa in pins + pouts:
             pa.free()
+        # the plain FP64 CG on the same workload, same run: the reference point of the speed-up
+        for _ in range(2):
+            fxs[0].zero()
+            D.solve(fbs[0], fxs[0], accuracy=w["tol"])
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        r64 = []
+        for k in range(args.steps):
+            fxs[0].zero()
+            r64.append(D.solve(fbs[k % nrhs], fxs[0], accuracy=w["tol"]))
+        ev1.record(stream)
+        ev1.synchronize()
+        t64 = dist.max(ev0.elapsed_time(ev1) * 1e-3)
+        fp64 = dist.world * args.steps / t64
+        result.update(fp64_solves_per_s=round(fp64, 3), speedup_vs_fp64=round(value / fp64, 3),
+                      fp64_iterations=r64[0].iterations, fp64_all_converged=all(r.converged for r in r64))
         roof_ms = dslash_time(50)
         result["dslash_ms_per_apply"] = roof_ms
         for f in fbs + fxs:
@@ -376,7 +402,7 @@ def run_ours(args, dist: Dist):
     }
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and args.workload != "dslash":
         cs = cpu_sample(args.workload)
-        iters = result.get("iterations") or 1
+        iters = result.get("fp64_iterations") or result.get("iterations") or 1
         out["cpu_baseline"] = {"value": 1.0 / (cs["t_iter"] * iters), "unit": "solves/s", "cores": cs["cores"],
                                "kind": "port",
                                "sample": f"{cs['iters']} CG iterations of the reference-structured oracle at "
@@ -397,12 +423,159 @@ def run_ours(args, dist: Dist):
     dist.close()
 
 
+# ------------------------------------------------------------------ serving
+
+def serve_stream(w, seed=11):
+    """The request stream: (arrival time s, lattice index, kappa, source indices)."""
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    lo, hi = w["nrhs_range"]
+    for n in range(w["requests"]):
+        t += rng.exponential(1.0 / w["rate"])
+        g = int(rng.integers(0, len(w["lattices"])))
+        nrhs = int(rng.integers(lo, hi + 1))
+        kappa = float(rng.uniform(*w["kappa_range"]))
+        reqs.append((t, g, kappa, [(n + k) % SERVE_POOL for k in range(nrhs)]))
+    return reqs
+
+
+SERVE_POOL = 6  # distinct sources generated per lattice; a request takes consecutive ones
+
+
+def pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(q * len(v)))] if v else None
+
+
+def run_serve(args, dist: Dist):
+    """Poisson request stream through the server, and the same stream through the FP64 CG (FIFO)."""
+    import torch
+    import hila_b200 as hw
+    torch.cuda.set_device(dist.local_rank)
+    dist.init("nccl")
+    w = WORKLOADS["serve"]
+    ctx = hw.Context(dist.local_rank)
+    reqs = serve_stream(w, seed=11 + dist.rank)
+    lats, gauges, pools = [], [], []
+    for i, dims in enumerate(w["lattices"]):
+        lat = hw.Lattice(ctx, dims, True)
+        lats.append(lat)
+        gauges.append(hw.GaugeField(lat, hw.generate_links(dims, w["eps"], w["link_seed"] + i), args.link_format))
+        pools.append([hw.generate_spinor(dims, w["src_seed"] + 100 * i + k, hw.EVEN) for k in range(SERVE_POOL)])
+    srv = hw.Server(ctx, precision=args.precision, delta=args.delta)
+    gids = [srv.add_gauge(G) for G in gauges]
+    # warm-up: one request per lattice (graphs and tables built, memory pools grown)
+    for g in range(len(lats)):
+        rid = srv.submit(gids[g], w["kappa"], [pools[g][0]], w["tol"])
+        srv.wait(rid, 1, lats[g].volume, copy=False)
+    out_pool = [[np.zeros((lat.volume, 4, 3, 2)) for _ in range(w["nrhs_range"][1])] for lat in lats]
+    st0 = srv.stats()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local_rank)
+    clocks.start()
+    ids, t_sub = [None] * len(reqs), [0.0] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for n, (ta, g, kappa, src) in enumerate(reqs):
+            d = t0 + ta - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            t_sub[n] = time.perf_counter()
+            ids[n] = srv.submit(gids[g], kappa, [pools[g][k] for k in src], w["tol"])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    results, t_done = [None] * len(reqs), [0.0] * len(reqs)
+    for n, (ta, g, kappa, src) in enumerate(reqs):
+        while ids[n] is None:
+            time.sleep(1e-4)
+        sols, res = srv.wait(ids[n], len(src), lats[g].volume, copy=False)
+        t_done[n] = t_sub[n] + res.latency_seconds
+        results[n] = res
+    th.join()
+    clk = clocks.stop()
+    st = srv.stats()
+    t_wall = max(t_done) - t0
+    solves = sum(len(r[3]) for r in reqs)
+    value = dist.sum(solves / t_wall)
+    lat_ms = [1e3 * r.latency_seconds for r in results]
+    ok = all(r.converged for r in results)
+    # correctness spot check: a solution through the public API against the FP64 true residual
+    g_chk = len(lats) - 1
+    rid = srv.submit(gids[g_chk], w["kappa"], [pools[g_chk][0]], w["tol"])
+    sols, r_chk = srv.wait(rid, 1, lats[g_chk].volume)
+    D_chk = hw.Dirac_Wilson_evenodd(w["kappa"], gauges[g_chk])
+    srv.close()
+    fx, fy = hw.Field(lats[g_chk], sols[0]), hw.Field(lats[g_chk])
+    D_chk.apply(fx, fy)
+    b0 = pools[g_chk][0]
+    chk = float(np.linalg.norm(fy.download(hw.EVEN) - b0) / np.linalg.norm(b0))
+    fx.close()
+    fy.close()
+    # the same stream served by the plain FP64 CG, one source at a time, in arrival order: the
+    # service time of every request is measured, the FIFO queue is then exact arithmetic
+    for g in range(len(lats)):
+        hw.Dirac_Wilson_evenodd(w["kappa"], gauges[g]).solve_host(pools[g][0], out_pool[g][0], accuracy=w["tol"])
+    torch.cuda.synchronize()
+    t_free, lat64, busy, ok64 = 0.0, [], 0.0, True
+    for (ta, g, kappa, src) in reqs:
+        D = hw.Dirac_Wilson_evenodd(kappa, gauges[g])
+        s0 = time.perf_counter()
+        for j, k in enumerate(src):
+            ok64 &= D.solve_host(pools[g][k], out_pool[g][j], accuracy=w["tol"]).converged
+        dt = time.perf_counter() - s0
+        busy += dt
+        start = max(ta, t_free)
+        t_free = start + dt
+        lat64.append(1e3 * (t_free - ta))
+    fifo_rate = solves / t_free  # wall rate of the FIFO schedule of this stream
+    fifo_capacity = solves / busy
+    out = {
+        "metric": "served CG solves/s at 1e-10 residual (Poisson stream, 8 lattices)", "value": round(value, 4),
+        "unit": "solves/s", "n_gpus": dist.world, "steps": len(reqs), "warmup": len(lats),
+        "ms_per_step": round(1e3 * t_wall / len(reqs), 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"f32": "f32+f64", "f16": "f16+f64"}[args.precision],
+        "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources, Poisson arrivals",
+        "config": {"workload": "serve", "lattices": ["x".join(map(str, d)) for d in w["lattices"]],
+                   "requests": len(reqs), "rate_per_s": w["rate"], "nrhs_range": w["nrhs_range"],
+                   "kappa_range": w["kappa_range"], "tol": w["tol"], "link_format": args.link_format,
+                   "precision": args.precision, "delta": args.delta, "parallelism": f"replicas{dist.world}"},
+        "e2e": {"value": round(value, 4), "unit": "solves/s", "note": "host arrays in and out through the server",
+                "h2d_bytes_per_step": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs)),
+                "d2h_bytes_per_step": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs))},
+        "latency_ms_p50": pct(lat_ms, 0.5), "latency_ms_p99": pct(lat_ms, 0.99),
+        "queue_ms_p50": pct([1e3 * r.queue_seconds for r in results], 0.5),
+        "all_converged": ok, "max_true_residual": max(r.true_residual for r in results),
+        "spot_check_residual": chk, "solves": solves, "wall_s": round(t_wall, 3),
+        "fifo_f64": {"solves_per_s": round(fifo_rate, 3), "capacity_solves_per_s": round(fifo_capacity, 3),
+                     "latency_ms_p50": pct(lat64, 0.5), "latency_ms_p99": pct(lat64, 0.99),
+                     "all_converged": ok64},
+        "server_stats": {k: st[k] for k in ("completed", "solves_completed", "rejected", "cancelled")},
+        "gpu_launches": int(st["kernel_launches"] - st0["kernel_launches"]),
+        "chunks": int(st["chunks"] - st0["chunks"]), "clocks": clk, "impl": "ours",
+    }
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+    for G in gauges:
+        G.close()
+    for lat in lats:
+        lat.close()
+    ctx.close()
+    dist.close()
+
+
 # ------------------------------------------------------------------ reference arm
 
 def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return
     w = WORKLOADS[args.workload]
+    if args.workload == "serve":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; its FP64 CG "
+                          "is timed on the cg and mrhs workloads"}), flush=True)
+        return
     if args.workload == "dslash":
         samples = [cpu_sample("cg", seconds_budget=2.0) for _ in range(args.warmup + args.steps)][args.warmup:]
         t = statistics.mean(s["t_apply"] for s in samples)
@@ -436,16 +609,28 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="cg", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mrhs", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
-    ap.add_argument("--link-format", type=int, default=18, choices=[18, 12])
+    ap.add_argument("--precision", default=None, choices=["f64", "f32", "f16"],
+                    help="default: f16 for mrhs/serve, f64 otherwise")
+    ap.add_argument("--link-format", type=int, default=12, choices=[18, 12])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="CG iterations from a host loop (for launch lists)")
-    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update factor of the mixed-precision solves")
+    ap.add_argument("--delta", type=float, default=None,
+                    help="reliable-update factor of the mixed-precision solves (default 0.005 FP16, 1e-5 FP32)")
     ap.add_argument("--lattice", default=None, help="override the workload's lattice, e.g. 24x24x24x24")
     ap.add_argument("--nrhs", type=int, default=None, help="override the right-hand sides per step (mrhs)")
+    ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=None, help="serve: Poisson arrival rate (requests/s)")
     args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "f16" if args.workload in ("mrhs", "serve") else "f64"
+    if args.delta is None:
+        args.delta = 1e-5 if args.precision == "f32" else 0.005
+    if args.requests:
+        WORKLOADS["serve"]["requests"] = args.requests
+    if args.rate:
+        WORKLOADS["serve"]["rate"] = args.rate
     if args.lattice:
         WORKLOADS[args.workload]["dims"] = tuple(int(v) for v in args.lattice.split("x"))
     if args.nrhs:
@@ -457,6 +642,8 @@ def main():
     dist = Dist()
     if args.impl == "reference":
         run_reference(args, dist)
+    elif args.workload == "serve":
+        run_serve(args, dist)
     else:
         run_ours(args, dist)
 

@@ -72,6 +72,26 @@ class _CgResult(ctypes.Structure):
                 ("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_int)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("delta", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("chunk_iters", ctypes.c_int)]
+
+
+class _RequestResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("nrhs", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("reliable_updates", ctypes.c_int), ("true_residual", ctypes.c_double),
+                ("latency_seconds", ctypes.c_double), ("queue_seconds", ctypes.c_double)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64), ("running", ctypes.c_uint64), ("queued", ctypes.c_uint64),
+                ("bytes_in_use", ctypes.c_size_t), ("bytes_budget", ctypes.c_size_t),
+                ("latency_p50_seconds", ctypes.c_double), ("latency_p99_seconds", ctypes.c_double),
+                ("solves_completed", ctypes.c_uint64), ("chunks", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64)]
+
+
 class _SolveRequest(ctypes.Structure):
     _fields_ = [("gauge", ctypes.c_void_p), ("kappa", ctypes.c_double), ("b", ctypes.c_void_p),
                 ("x", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int)]
@@ -115,6 +135,15 @@ _SIGNATURES = {
                                                        ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
     "hw_batch_solve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_SolveRequest),
                                       ctypes.c_int, ctypes.POINTER(_CgResult)]),
+    "hw_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(_ServerConfig), ctypes.POINTER(_vp)]),
+    "hw_server_destroy": (ctypes.c_int, [_vp]),
+    "hw_server_add_gauge": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int)]),
+    "hw_server_submit": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_dp),
+                                        ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
+    "hw_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(_dp), ctypes.c_double,
+                                      ctypes.POINTER(_RequestResult)]),
+    "hw_server_cancel": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "hw_server_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(_ServerStats)]),
     "hw_generate_links": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_uint64, _dp]),
     "hw_generate_spinor": (ctypes.c_int, [_ip, ctypes.c_uint64, ctypes.c_int, _dp]),
 }
@@ -211,13 +240,29 @@ class PinnedArray:
 
 # ------------------------------------------------------------------ handles
 
+def _close_children(children):
+    for ref in reversed(children):
+        obj = ref()
+        if obj is not None:
+            obj.close()
+
+
 class Context:
-    """One GPU (stream, reduction buffers, graph caches)."""
+    """One GPU (stream, reduction buffers, graph caches).
+
+    Handles made on a context (lattices, gauge and spinor fields, servers)
+    register here; close() releases them first, newest first, so no handle can
+    reach the C context after it is gone."""
 
     def __init__(self, device: int = 0):
         self.handle = _vp()
         _check(lib().hw_context_create(int(device), ctypes.byref(self.handle)))
         self.device = device
+        self._children = []
+
+    def _adopt(self, obj):
+        import weakref
+        self._children.append(weakref.ref(obj))
 
     def synchronize(self):
         _check(lib().hw_context_synchronize(self.handle))
@@ -230,6 +275,8 @@ class Context:
 
     def close(self):
         if self.handle:
+            _close_children(self._children)
+            self._children = []
             lib().hw_context_destroy(self.handle)
             self.handle = _vp()
 
@@ -241,7 +288,8 @@ class Context:
 
 
 class Lattice:
-    """lattice.setup(dims) (plumbing/lattice.cpp:37-104); t antiperiodic for fermions."""
+    """lattice.setup(dims) (plumbing/lattice.cpp:37-104); t antiperiodic for fermions.
+    close() first releases the gauge and spinor fields made on it."""
 
     def __init__(self, ctx: Context, dims, antiperiodic: bool = True):
         self.ctx = ctx
@@ -250,9 +298,18 @@ class Lattice:
         self.handle = _vp()
         _check(lib().hw_lattice_create(ctx.handle, _dims(self.dims), int(bool(antiperiodic)),
                                        ctypes.byref(self.handle)))
+        self._children = []
+        ctx._adopt(self)
+
+    def _adopt(self, obj):
+        import weakref
+        self._children.append(weakref.ref(obj))
+        self.ctx._adopt(obj)
 
     def close(self):
         if self.handle:
+            _close_children(self._children)
+            self._children = []
             lib().hw_lattice_destroy(self.handle)
             self.handle = _vp()
 
@@ -274,6 +331,7 @@ class GaugeField:
         self.link_format = link_format
         self.handle = _vp()
         _check(lib().hw_gauge_create(lattice.handle, _dptr(links), int(link_format), ctypes.byref(self.handle)))
+        lattice._adopt(self)
 
     def close(self):
         if self.handle:
@@ -294,6 +352,7 @@ class Field:
         self.lattice = lattice
         self.handle = _vp()
         _check(lib().hw_field_create(lattice.handle, ctypes.byref(self.handle)))
+        lattice._adopt(self)
         if data is not None:
             self.upload(data, parity)
 
@@ -481,3 +540,80 @@ def wilson_evenodd_apply_noalloc(dims, kappa: float, sign: int, links_ptr: int, 
     _check(lib().hw_wilson_evenodd_apply_noalloc(_dims(dims), int(bool(antiperiodic)), float(kappa), int(sign),
                                                  _vp(links_ptr), int(link_format), _vp(in_ptr), _vp(out_ptr),
                                                  int(stride), _vp(stream)))
+
+
+@dataclass
+class RequestResult:
+    status: int
+    nrhs: int
+    iterations: int
+    reliable_updates: int
+    true_residual: float
+    latency_seconds: float
+    queue_seconds: float
+
+    @property
+    def converged(self) -> bool:
+        return self.status == HW_OK
+
+
+class Server:
+    """Continuous-batching solve server (hw_server_*).
+
+    Submit requests from any thread; gauge fields stay on the device; requests
+    that arrive while others run join at the next chunk; every result is
+    bitwise the same alone and in any mix."""
+
+    def __init__(self, ctx: Context, precision: str = "f16", delta: float = 0.0, hbm_budget_bytes: int = 0,
+                 chunk_iters: int = 8):
+        cfg = _ServerConfig(PRECISIONS[precision], float(delta), int(hbm_budget_bytes), int(chunk_iters))
+        self.ctx = ctx
+        self.handle = _vp()
+        _check(lib().hw_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(self.handle)))
+        ctx._adopt(self)
+
+    def add_gauge(self, gauge: GaugeField) -> int:
+        gid = ctypes.c_int()
+        _check(lib().hw_server_add_gauge(self.handle, gauge.handle, ctypes.byref(gid)))
+        return gid.value
+
+    def submit(self, gauge_id: int, kappa: float, sources, accuracy: float = 1e-10, maxiters: int = 10000) -> int:
+        srcs = [np.ascontiguousarray(s_, np.float64) for s_ in sources]
+        arr = (_dp * len(srcs))(*[_dptr(s_) for s_ in srcs])
+        rid = ctypes.c_uint64()
+        _check(lib().hw_server_submit(self.handle, int(gauge_id), float(kappa), len(srcs), arr, float(accuracy),
+                                      int(maxiters), ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, request_id: int, nrhs: int, volume: int, timeout: float = -1.0, copy: bool = True):
+        """Returns (solutions, RequestResult); solutions is a list of (V,4,3,2)
+        arrays, or None with copy=False."""
+        sols, arr = None, None
+        if copy:
+            sols = [np.zeros((volume, 4, 3, 2), np.float64) for _ in range(nrhs)]
+            arr = (_dp * nrhs)(*[_dptr(s_) for s_ in sols])
+        r = _RequestResult()
+        rc = lib().hw_server_wait(self.handle, ctypes.c_uint64(request_id), arr, float(timeout), ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_CANCELLED, HW_ERR_REJECTED):
+            _check(rc)
+        return sols, RequestResult(r.status, r.nrhs, r.iterations, r.reliable_updates, r.true_residual,
+                                   r.latency_seconds, r.queue_seconds)
+
+    def cancel(self, request_id: int) -> None:
+        _check(lib().hw_server_cancel(self.handle, ctypes.c_uint64(request_id)))
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(lib().hw_server_stats_get(self.handle, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().hw_server_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

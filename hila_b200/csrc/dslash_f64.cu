@@ -320,7 +320,28 @@ __global__ void k_links_lex_to_eo(Geom g, const double2 *lex_dir, double2 *dst, 
     for (int k = 0; k < nplanes; k++) dst[(size_t)k * stride + i] = src[k];
 }
 
+// checkerboard-ordered AoS [Vh][12] complex <-> SoA planes of one parity
+__global__ void k_aos_to_soa(int n, const double2 *aos, SpinorF64 out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < 12; c++) out.p[(size_t)c * out.stride + i] = aos[(size_t)i * 12 + c];
+}
+__global__ void k_soa_to_aos(int n, SpinorF64 in, double2 *aos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < 12; c++) aos[(size_t)i * 12 + c] = in.p[(size_t)c * in.stride + i];
+}
+
 }  // namespace
+
+void launch_aos_to_soa(int n, const double *aos, HalfF64 out, cudaStream_t s) {
+    k_aos_to_soa<<<(n + 255) / 256, 256, 0, s>>>(n, reinterpret_cast<const double2 *>(aos), sp(out));
+}
+void launch_soa_to_aos(int n, HalfF64 in, double *aos, cudaStream_t s) {
+    k_soa_to_aos<<<(n + 255) / 256, 256, 0, s>>>(n, sp(in), reinterpret_cast<double2 *>(aos));
+}
 
 // ------------------------------------------------------------------ launchers
 

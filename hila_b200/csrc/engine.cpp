@@ -43,6 +43,7 @@ Engine::~Engine() {
     }
     if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
     if (pinned_states_) cudaFreeHost(pinned_states_);
+    if (pinned_ctl_) cudaFreeHost(pinned_ctl_);
 }
 
 int Engine::init() {
@@ -55,6 +56,7 @@ int Engine::init() {
     HW_CUDA(cudaMemsetAsync(d_tickets_.ptr, 0, d_tickets_.bytes, ctx_->stream));
     HW_CUDA(cudaMemsetAsync(d_ctl_.ptr, 0, d_ctl_.bytes, ctx_->stream));
     HW_CUDA(cudaMallocHost(&pinned_states_, sizeof(EngState) * kEngMaxProb));
+    HW_CUDA(cudaMallocHost(&pinned_ctl_, sizeof(int) * 8));
     std::memset(&tables_, 0, sizeof(tables_));
     for (int j = 0; j < kEngMaxProb; j++) {
         std::memset(&host_states_[j], 0, sizeof(EngState));
@@ -170,11 +172,14 @@ int Engine::free_slots_on(int lat) const {
     return std::min(kEngMaxRhs - used, free_total);
 }
 
-size_t Engine::slot_bytes(int lat) const {
-    const size_t st = tables_.lat[lat].stride;
+size_t Engine::slot_bytes_for_stride(int stride) const {
+    const size_t st = stride;
     const size_t low_site = low_ == LOW_F16 ? (48 + 4) : 96;
-    return st * (4 * low_site + 96 + 2 * 192) + st * 2 * 192;  // + owned x, b
+    // p, r, Dp, t (low) + y (FP32) + s, t64 (FP64) + owned x, b (FP64)
+    return st * (4 * low_site + 96 + 2 * 192) + st * 2 * 192;
 }
+
+size_t Engine::slot_bytes(int lat) const { return slot_bytes_for_stride(tables_.lat[lat].stride); }
 
 int Engine::ensure_slot_buffers(int slot, int stride) {
     SlotBuffers &B = bufs_[slot];
@@ -384,8 +389,10 @@ int Engine::launch_chunk(int iters) {
 int Engine::read_states() {
     HW_CUDA(cudaMemcpyAsync(pinned_states_, d_states_.ptr, sizeof(EngState) * kEngMaxProb, cudaMemcpyDeviceToHost,
                             ctx_->stream));
+    HW_CUDA(cudaMemcpyAsync(pinned_ctl_, d_ctl_.ptr, sizeof(int) * 8, cudaMemcpyDeviceToHost, ctx_->stream));
     HW_CUDA(cudaStreamSynchronize(ctx_->stream));
     HW_CUDA(cudaGetLastError());
+    bodies_total_ = reinterpret_cast<const unsigned long long *>(pinned_ctl_ + 6)[0];
     for (int j = 0; j < kEngMaxProb; j++)
         if (slots_[j].used) host_states_[j] = pinned_states_[j];
     return HW_OK;

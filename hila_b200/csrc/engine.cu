@@ -503,6 +503,7 @@ __global__ void k_eng_control(EngPtrs P, int nprob, int chunk, cudaGraphConditio
         P.ctl[0] = it;
         P.ctl[1] = running;
         P.ctl[2] = 0;  // pending reliable updates were served this iteration
+        reinterpret_cast<unsigned long long *>(P.ctl + 6)[0] += 1;  // loop bodies since init
         if (use_cond) cudaGraphSetConditional(h, (running > 0 && it < chunk) ? 1u : 0u);
     }
 }

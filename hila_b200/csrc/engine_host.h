@@ -45,10 +45,15 @@ class Engine {
     int launch_chunk(int iters);
     // copy the slot states to the host mirror (synchronises the stream)
     int read_states();
+    // loop bodies (10 phase kernels + 1 control kernel each) run since init, as of the last read_states
+    unsigned long long bodies_total() const { return bodies_total_; }
     const EngState &state(int slot) const { return host_states_[slot]; }
     void release(int slot);
     int nslots_used() const;
     size_t slot_bytes(int lat) const;
+    // device bytes of one solve slot (including slot-owned b and x) for a lattice stride
+    size_t slot_bytes_for_stride(int stride) const;
+    int slot_lattice(int slot) const { return slots_[slot].lat; }
     const EngLattice &lattice(int l) const { return tables_.lat[l]; }
     int nlat() const { return tables_.nlat; }
     const hw_gauge *gauge(int l) const { return gauges_[l]; }
@@ -70,6 +75,8 @@ class Engine {
     SlotBuffers bufs_[kEngMaxProb];
     EngState host_states_[kEngMaxProb];
     EngState *pinned_states_ = nullptr;
+    int *pinned_ctl_ = nullptr;
+    unsigned long long bodies_total_ = 0;
     DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_;
     size_t partial_tiles_ = 0;
     EngGrid grid_{};

@@ -79,6 +79,9 @@ void launch_scale(int Vh, HalfF64 x, HalfF64 y, double a, cudaStream_t s);
 // ---- layout conversion (host canonical lexicographic AoS <-> device even-odd SoA)
 void launch_spinor_lex_to_eo(const Geom &g, const double *lex, int par, HalfF64 out, cudaStream_t s);
 void launch_spinor_eo_to_lex(const Geom &g, HalfF64 in, int par, double *lex, cudaStream_t s);
+// checkerboard-ordered AoS [n][12] complex <-> the SoA planes of one half lattice
+void launch_aos_to_soa(int n, const double *aos, HalfF64 out, cudaStream_t s);
+void launch_soa_to_aos(int n, HalfF64 in, double *aos, cudaStream_t s);
 // one direction of links [V][3][3] complex (lexicographic) -> the planes of (par, dir)
 void launch_links_lex_to_eo(const Geom &g, const double *lex_dir, double2 *dst, int nplanes, int stride, int par,
                             cudaStream_t s);

@@ -72,6 +72,8 @@ int hw_device_count(int *count);
 /* One context per GPU: owns the stream, reduction buffers and graph caches.
  * Replaces hila::initialize's device setup (libraries/plumbing/initialize.cpp). */
 int hw_context_create(int device, hw_context **ctx);
+/* Destroy servers, fields, gauge fields and lattices of a context before the
+ * context, and fields and gauge fields of a lattice before the lattice. */
 int hw_context_destroy(hw_context *ctx);
 int hw_context_synchronize(hw_context *ctx);
 /* The context's CUDA stream (a cudaStream_t), so callers can order their own
@@ -218,6 +220,62 @@ typedef struct hw_solve_request {
  * outcome; each solve gives bitwise the same result alone and in a batch. */
 int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_request *requests, int n,
                    hw_cg_result *results);
+
+/* ------------------------------------------------------------------ serving */
+
+/* A solve server over one context (no reference counterpart: HILA has no
+ * serving layer).  Gauge fields stay device resident; requests (gauge, kappa,
+ * 1..16 sources, accuracy) are queued by any thread and run by a server thread
+ * with continuous batching on the mixed-precision engine: between chunks of
+ * `chunk_iters` CG iterations it retires finished solves and admits waiting
+ * requests while others keep iterating, as long as the requests' solve memory
+ * fits `hbm_budget_bytes`.  Each solve's result is bitwise the same alone and
+ * in any mix. */
+typedef struct hw_server hw_server;
+
+typedef struct hw_server_config {
+    int precision;            /* HW_PREC_F16 (default) or HW_PREC_F32 inner solves */
+    double delta;             /* reliable-update factor (<= 0: 0.005 for FP16, 1e-5 for FP32) */
+    size_t hbm_budget_bytes;  /* device memory for solve slots (0: 80% of free memory at creation) */
+    int chunk_iters;          /* CG iterations between admission points (<= 0: 8) */
+} hw_server_config;
+
+typedef struct hw_request_result {
+    int status;               /* HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN, HW_ERR_CANCELLED, HW_ERR_REJECTED */
+    int nrhs;
+    int iterations;           /* largest iteration count over the request's sources */
+    int reliable_updates;     /* largest over the sources */
+    double true_residual;     /* largest |b - M x| / |b| over the sources (FP64) */
+    double latency_seconds;   /* submit -> result available */
+    double queue_seconds;     /* submit -> admitted */
+} hw_request_result;
+
+typedef struct hw_server_stats {
+    uint64_t submitted, completed, rejected, cancelled, running, queued;
+    size_t bytes_in_use, bytes_budget;
+    double latency_p50_seconds, latency_p99_seconds;  /* over completed requests */
+    uint64_t solves_completed;                         /* sources, not requests */
+    uint64_t chunks;                                   /* chunk graphs launched */
+    uint64_t kernel_launches;                          /* kernels those chunks ran */
+} hw_server_stats;
+
+int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server **server);
+int hw_server_destroy(hw_server *server);
+/* register a gauge field with the server (it must outlive the server) */
+int hw_server_add_gauge(hw_server *server, const hw_gauge *gauge, int *gauge_id);
+/* queue M x = b for nrhs host sources (canonical layout, EVEN sites used);
+ * the sources are copied before the call returns */
+int hw_server_submit(hw_server *server, int gauge_id, double kappa, int nrhs, const double *const *sources,
+                     double accuracy, int maxiters, uint64_t *request_id);
+/* wait up to timeout_seconds (< 0: forever) for a request; on completion copy
+ * its solutions (canonical layout, ODD sites zero) into solutions[0..nrhs-1]
+ * (solutions or an entry may be NULL) and fill *result.  HW_ERR_TIMEOUT if
+ * still running.  A finished request is forgotten after its wait. */
+int hw_server_wait(hw_server *server, uint64_t request_id, double *const *solutions, double timeout_seconds,
+                   hw_request_result *result);
+/* cancel a queued or running request (its slots are freed at the next chunk) */
+int hw_server_cancel(hw_server *server, uint64_t request_id);
+int hw_server_stats_get(hw_server *server, hw_server_stats *stats);
 
 /* ------------------------------------------------------------------ inputs */
 
