@@ -15,22 +15,33 @@ int ensure_low_links(const hw_gauge *G, int low, bool full18) {
     hw_context *ctx = lat->ctx;
     const size_t st = lat->stride;
     int rc;
-    if (full18) {
+    const double2 *l64 = G->f64.as<double2>();
+    const int planes = G->U().planes;
+    if (low == LOW_F32 && full18) {
         if (!G->f32a.ptr) {
             if ((rc = G->f32a.alloc(32 * st * sizeof(float4))) != HW_OK) return rc;
             if ((rc = G->f32b.alloc(8 * st * sizeof(float2))) != HW_OK) return rc;
-            eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, nullptr, nullptr, nullptr,
-                              G->f32a.as<float4>(), G->f32b.as<float2>(), ctx->stream);
+            eng_convert_links(lat->g, l64, planes, lat->stride, nullptr, nullptr, nullptr, G->f32a.as<float4>(),
+                              G->f32b.as<float2>(), nullptr, nullptr, ctx->stream);
         }
-    } else if (low == LOW_F32 && !G->f32.ptr) {
-        if ((rc = G->f32.alloc(24 * st * sizeof(float4))) != HW_OK) return rc;
-        eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, G->f32.as<float4>(), nullptr,
-                          nullptr, nullptr, nullptr, ctx->stream);
-    } else if (low == LOW_F16 && !G->f16a.ptr) {
+    } else if (low == LOW_F32) {
+        if (!G->f32.ptr) {
+            if ((rc = G->f32.alloc(24 * st * sizeof(float4))) != HW_OK) return rc;
+            eng_convert_links(lat->g, l64, planes, lat->stride, G->f32.as<float4>(), nullptr, nullptr, nullptr,
+                              nullptr, nullptr, nullptr, ctx->stream);
+        }
+    } else if (full18) {
+        if (!G->f16x.ptr) {
+            if ((rc = G->f16x.alloc(16 * st * sizeof(uint4))) != HW_OK) return rc;
+            if ((rc = G->f16z.alloc(8 * st * sizeof(unsigned))) != HW_OK) return rc;
+            eng_convert_links(lat->g, l64, planes, lat->stride, nullptr, nullptr, nullptr, nullptr, nullptr,
+                              G->f16x.as<uint4>(), G->f16z.as<unsigned>(), ctx->stream);
+        }
+    } else if (!G->f16a.ptr) {
         if ((rc = G->f16a.alloc(8 * st * sizeof(uint4))) != HW_OK) return rc;
         if ((rc = G->f16b.alloc(8 * st * sizeof(uint2))) != HW_OK) return rc;
-        eng_convert_links(lat->g, G->f64.as<double2>(), G->U().planes, lat->stride, nullptr, G->f16a.as<uint4>(),
-                          G->f16b.as<uint2>(), nullptr, nullptr, ctx->stream);
+        eng_convert_links(lat->g, l64, planes, lat->stride, nullptr, G->f16a.as<uint4>(), G->f16b.as<uint2>(),
+                          nullptr, nullptr, nullptr, nullptr, ctx->stream);
     }
     HW_CUDA(cudaGetLastError());
     return HW_OK;
@@ -63,10 +74,14 @@ int Engine::init() {
         host_states_[j].status = ENG_IDLE;
     }
     HW_CUDA(cudaMemcpyAsync(d_states_.ptr, host_states_, sizeof(host_states_), cudaMemcpyHostToDevice, ctx_->stream));
-    // inner links: the 12-real links of the inner precision by default (fewest bytes,
-    // measured fastest); HW_ENGINE_LINKS=18 selects 18-real FP32 links (no third-row rebuild)
+    // inner links: FP16 engines read all 18 reals (no third-row rebuild in the hop,
+    // measured fastest), FP32 engines the 12-real links (fewest bytes);
+    // HW_ENGINE_LINKS=12 / 18 overrides.  The tensor-core variant needs 18-real FP16 links.
+    full18_ = low_ == LOW_F16;
     if (const char *env = std::getenv("HW_ENGINE_LINKS")) full18_ = std::atoi(env) == 18;
-    grid_ = eng_grid_size(low_, kDefaultVariant, full18_ ? 1 : 0, 1);
+    if (const char *env = std::getenv("HW_ENGINE_VARIANT"))
+        if (std::atoi(env) == 4 && low_ == LOW_F16) full18_ = true;
+    grid_ = eng_grid_size(low_, default_variant(), full18_ ? 1 : 0, 1);
     // HW_USE_GRAPH=0 runs the iterations from a host loop instead of the captured
     // WHILE graph (profilers see the individual kernel launches)
     if (const char *env = std::getenv("HW_USE_GRAPH")) use_graph_ = std::atoi(env) != 0;
@@ -115,6 +130,8 @@ int Engine::lattice_index(const hw_gauge *G, int *idx) {
     L.l16b = G->f16b.as<uint2>();
     L.l32a = G->f32a.as<float4>();
     L.l32b = G->f32b.as<float2>();
+    L.l16x = G->f16x.as<uint4>();
+    L.l16z = G->f16z.as<unsigned>();
     tables_.ntiles += L.ntiles;
     tables_.max_tiles = std::max(tables_.max_tiles, L.ntiles);
     tables_.nlat = l + 1;
@@ -350,9 +367,10 @@ int Engine::configure() {
     int mask = 0;
     for (int l = 0; l < tables_.nlat; l++) mask |= tables_.lat[l].l64_planes == 9 ? 1 : 2;
     if (mask == 0) mask = 1;
-    int variant = kDefaultVariant;
+    int variant = default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
-    if (variant < 0 || variant > 3) variant = kDefaultVariant;
+    // the tensor-core variant reads the 18-real FP16 links, which exist only with full18_
+    if (variant < 0 || variant > 4 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
     if (variant != grid_.variant || mask != grid_.planes_mask) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
         if (chunk_exec_) {

@@ -6,6 +6,8 @@
 // summed per slot in tile order by the last block to finish the lattice, so a
 // slot's arithmetic does not depend on which other slots share the launch:
 // a solve gives bitwise the same result alone and inside any batch.
+#include <cuda_fp16.h>
+
 #include <type_traits>
 
 #include "engine.h"
@@ -39,16 +41,22 @@ struct Low<LOW_F16> {
     static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l16a, L.l16b, L.stride}; }
 };
 
-// links of the inner phases: the precision's own 12-real format, or 18-real FP32
+// links of the inner phases: the precision's own 12-real format, or all 18 reals
+// in the precision (no third-row rebuild)
 template <int LOW, bool FULL18>
 struct InnerLinks {
     using Lk = typename Low<LOW>::Lk;
     static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Low<LOW>::lk(L); }
 };
-template <int LOW>
-struct InnerLinks<LOW, true> {
+template <>
+struct InnerLinks<LOW_F32, true> {
     using Lk = LinksF32x18;
     static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l32a, L.l32b, L.stride}; }
+};
+template <>
+struct InnerLinks<LOW_F16, true> {
+    using Lk = LinksF16x18;
+    static __device__ __forceinline__ Lk lk(const EngLattice &L) { return Lk{L.l16x, L.l16z, L.stride}; }
 };
 
 __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
@@ -287,6 +295,8 @@ __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLat
     __syncthreads();
 }
 
+#include "engine_mma.cuh"
+
 // Inner phases P1..P4 in low precision.  Each thread owns one site and up to
 // NR right-hand sides at a time, so links, their third rows and the neighbour
 // indices are shared by the NR solves.
@@ -408,15 +418,16 @@ __global__ void __launch_bounds__(kEngTile, 2) k_eng_f64(EngPtrs P) {
                 double red[2] = {0.0, 0.0};
                 if (valid) {
                     const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
-                    const SpinorF64 sin[1] = {SpinorF64{const_cast<double2 *>(in), stride}};
-                    Spinor<double> acc[1];
+                    const SpinorF64 sin{const_cast<double2 *>(in), stride};
+                    Spinor<double> acc;
 #pragma unroll
-                    for (int c = 0; c < 12; c++) acc[0].s[c / 3][c % 3] = {0.0, 0.0};
-                    hop_dir_multi<0, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
-                    hop_dir_multi<1, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
-                    hop_dir_multi<2, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
-                    hop_dir_multi<3, SIGN>(nb, OUTPAR, i, sin, 1, U, acc);
-                    epi_f64<PHASE, LOW>(pr, stride, i, acc[0], red);
+                    for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {0.0, 0.0};
+                    // spinor first, link second: fewer values live than the multi-source hop
+                    hop_dir<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                    hop_dir<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                    hop_dir<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                    hop_dir<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                    epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
                 }
                 if constexpr (NRED > 0) {
 #pragma unroll
@@ -512,12 +523,28 @@ __global__ void k_eng_chunk_begin(EngPtrs P) { P.ctl[0] = 0; }
 
 // FP64 link planes (first six elements = rows 0 and 1) -> FP32 / FP16 12-real planes
 __global__ void k_eng_links(Geom g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                            uint2 *l16b, float4 *l32a, float2 *l32b) {
+                            uint2 *l16b, float4 *l32a, float2 *l32b, uint4 *l16x, unsigned *l16z) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int pd = blockIdx.y;  // parity*4 + dir
     if (i >= g.Vh) return;
-    if (l32a) {
+    if (l16x) {
         // all 18 reals; a 12-real FP64 source gets its third row rebuilt in FP64 first
+        Su3<double> u;
+        for (int k = 0; k < 9; k++) {
+            if (k < planes) {
+                double2 v = l64[((size_t)pd * planes + k) * stride + i];
+                u.e[k / 3][k % 3] = {v.x, v.y};
+            }
+        }
+        if (planes == 6) reconstruct_row2(u);
+        __half2 h[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) h[k] = __floats2half2_rn((float)u.e[k / 3][k % 3].re, (float)u.e[k / 3][k % 3].im);
+        l16x[(size_t)(2 * pd) * stride + i] = *reinterpret_cast<const uint4 *>(&h[0]);
+        l16x[(size_t)(2 * pd + 1) * stride + i] = *reinterpret_cast<const uint4 *>(&h[4]);
+        l16z[(size_t)pd * stride + i] = *reinterpret_cast<const unsigned *>(&h[8]);
+    }
+    if (l32a) {
         Su3<double> u;
         for (int k = 0; k < 9; k++) {
             if (k < planes) {
@@ -581,14 +608,35 @@ void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
     k_eng_vec<PH_P5, LOW><<<G.low, kEngTile, 0, s>>>(P);
 }
 
+constexpr int kMmaMinBlocks = 4;
+
+// FP16 inner phases on the tensor cores (engine_mma.cuh), the rest as usual
+void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    k_eng_mma<PH_P1, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_mma<PH_P2, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_mma<PH_P3, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_mma<PH_P4, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_vec<PH_R1, LOW_F16><<<G.low, kEngTile, 0, s>>>(P);
+    launch_f64<PH_R2, LOW_F16>(P, G, s);
+    launch_f64<PH_R3, LOW_F16>(P, G, s);
+    launch_f64<PH_R4, LOW_F16>(P, G, s);
+    launch_f64<PH_R5, LOW_F16>(P, G, s);
+    k_eng_vec<PH_P5, LOW_F16><<<G.low, kEngTile, 0, s>>>(P);
+}
+
 // Launch shapes of the low-precision phases (EngGrid::variant):
 //   0: one right-hand side per thread, <= 128 registers (4 blocks of 128 per SM)
 //   1: one right-hand side per thread, <= 102 registers (5 blocks)
 //   2: one right-hand side per thread, <= 85 registers (6 blocks)
 //   3: two right-hand sides per thread sharing the links, <= 128 registers
-// each with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
+//   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
+// variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    if (LOW == LOW_F16 && G.variant == 4) {
+        enqueue_iteration_mma(P, G, s);
+        return;
+    }
     switch (G.variant) {
     case 1:
         enqueue_iteration_t<LOW, 1, 5, FULL18>(P, G, s);
@@ -630,9 +678,9 @@ void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphCondit
 void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s) { k_eng_chunk_begin<<<1, 1, 0, s>>>(P); }
 
 void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                       uint2 *l16b, float4 *l32a, float2 *l32b, cudaStream_t s) {
+                       uint2 *l16b, float4 *l32a, float2 *l32b, uint4 *l16x, unsigned *l16z, cudaStream_t s) {
     dim3 grid((g.Vh + 255) / 256, 8);
-    k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b, l32a, l32b);
+    k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b, l32a, l32b, l16x, l16z);
 }
 
 template <int LOW, int NR, int MINB>
@@ -644,6 +692,11 @@ int occupancy_low() {
 
 template <int LOW>
 int occupancy_variant(int v) {
+    if (LOW == LOW_F16 && v == 4) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_eng_mma<PH_P4, kMmaMinBlocks>, kEngTile, 0);
+        return n < 1 ? 1 : n;
+    }
     switch (v) {
     case 1:
         return occupancy_low<LOW, 1, 5>();

@@ -54,6 +54,8 @@ struct EngLattice {
     const uint2 *l16b;   // ... + 4 halves per link
     const float4 *l32a;  // FP32, 18 reals: 4 float4 planes ...
     const float2 *l32b;  // ... + 1 float2 plane per (parity, dir)
+    const uint4 *l16x;     // FP16, 18 reals: elements 0..7 in 2 uint4 planes ...
+    const unsigned *l16z;  // ... + element 8 in 1 plane per (parity, dir)
 };
 
 struct EngProblem {
@@ -112,7 +114,7 @@ struct EngGrid {
     int low;  // blocks of the low-precision phases (all SMs x resident blocks)
     int f64;  // blocks of the FP64 reliable-update phases
     int variant;  // launch shape of the low-precision phases (engine.cu)
-    int full18;   // 1: inner phases read 18-real FP32 links; 0: the 12-real links of the precision
+    int full18;   // 1: inner phases read 18-real links (FP32 or FP16); 0: the 12-real links of the precision
     int planes_mask;  // FP64 link formats present: bit 0 = 18 reals, bit 1 = 12 reals
 };
 
@@ -129,7 +131,7 @@ void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphCondit
 void eng_enqueue_chunk_begin(const EngPtrs &P, cudaStream_t s);
 // Convert FP64 link planes to the 12-real FP32 / FP16 planes of the inner solve.
 void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,
-                       uint2 *l16b, float4 *l32a, float2 *l32b, cudaStream_t s);
+                       uint2 *l16b, float4 *l32a, float2 *l32b, uint4 *l16x, unsigned *l16z, cudaStream_t s);
 // launch configuration of the engine kernels on the current device
 EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask);
 

@@ -86,7 +86,7 @@ class Engine {
     bool use_graph_ = true;
     bool full18_ = false;
     // launch shape of the inner phases (engine.cu): one RHS per thread, 6 blocks per SM
-    static constexpr int kDefaultVariant = 2;
+    int default_variant() const { return 2; }
 };
 
 // per-context engine for a low precision (LOW_F32 / LOW_F16), created on first use

@@ -130,7 +130,7 @@ struct hw_gauge {
     hw::DevBuf f64;  // FP64 planes
     hw::GaugeF64 U() const { return hw::GaugeF64{f64.as<double2>(), lat->stride, link_format == 12 ? 6 : 9}; }
     // low-precision copies for mixed-precision solves (built on first use)
-    mutable hw::DevBuf f32, f16a, f16b, f32a, f32b;
+    mutable hw::DevBuf f32, f16a, f16b, f32a, f32b, f16x, f16z;
 };
 
 struct hw_field {

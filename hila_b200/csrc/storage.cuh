@@ -240,6 +240,30 @@ struct LinksF16x12 {
     }
 };
 
+// All 18 reals in FP16: elements 0..7 in two uint4 planes, element 8 in one
+// 32-bit plane per (parity, dir).  No third-row rebuild in the hop.
+struct LinksF16x18 {
+    using R = float;
+    const uint4 *p;      // 2 planes per (parity, dir)
+    const unsigned *q;   // 1 plane per (parity, dir)
+    int stride;
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
+        const int pd = par * 4 + dir;
+        uint4 a[2];
+        a[0] = __ldg(p + (size_t)(2 * pd) * stride + i);
+        a[1] = __ldg(p + (size_t)(2 * pd + 1) * stride + i);
+        unsigned b = __ldg(q + (size_t)pd * stride + i);
+        const __half2 *ha = reinterpret_cast<const __half2 *>(a);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            float2 f = __half22float2(ha[k]);
+            u.e[k / 3][k % 3] = {f.x, f.y};
+        }
+        float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&b));
+        u.e[2][2] = {f.x, f.y};
+    }
+};
+
 // ------------------------------------------------------------------ hopping term
 //
 // acc = (H_s in)(x) for checkerboard site i of parity par (the output parity);
