@@ -202,6 +202,22 @@ def cpu_sample(workload: str, seconds_budget: float = 20.0):
 
 # ------------------------------------------------------------------ our arm
 
+def engine_phase_bytes(phase: str, vh: int, nrhs: int, prec: str, link_format: int) -> int:
+    """Algorithmic bytes of one engine phase launch: every array read or written once.
+
+    Low-precision spinor: FP16 48 B + 4 B norm, FP32 96 B; links of the inner phases:
+    all 4 V links once (FP16 18 reals, 36 B; FP32 12 reals, 48 B); y (FP32 96 B); FP64
+    spinor 192 B and FP64 links (144 or 96 B) in the reliable update."""
+    sp = 52 if prec == "f16" else 96
+    lk = 8 * (36 if prec == "f16" else 48)
+    lk64 = 8 * (144 if link_format == 18 else 96)
+    per = {"P1": (2 * sp, lk), "P2": (3 * sp, lk), "P3": (2 * sp, lk), "P4": (6 * sp + 2 * 96, lk),
+           "R1": (2 * 192 + 2 * 96, 0), "R2": (2 * 192, lk64), "R3": (4 * 192, lk64),
+           "R4": (2 * 192, lk64), "R5": (2 * 192 + sp, lk64), "P5": (3 * sp, 0)}
+    pair, links = per[phase]
+    return int(vh * (nrhs * pair + links))
+
+
 def run_ours(args, dist: Dist):
     import torch
     import hila_b200 as hw
@@ -336,6 +352,15 @@ def run_ours(args, dist: Dist):
                       fp64_iterations=r64[0].iterations, fp64_all_converged=all(r.converged for r in r64))
         roof_ms = dslash_time(50)
         result["dslash_ms_per_apply"] = roof_ms
+        # per-phase device time of one more batch (events around every engine launch)
+        ctx.engine_profile(True)
+        batch_once()
+        prof = ctx.engine_profile_get(prec)
+        ctx.engine_profile(False)
+        result["phases"] = {k: {"launches": n, "ms_per_launch": round(ms / n, 4) if n else None,
+                                "bytes_per_launch": engine_phase_bytes(k, V // 2, nrhs, prec, args.link_format)}
+                            for k, (n, ms) in prof.items()}
+        engine_roof = result["phases"]["P4"]
         for f in fbs + fxs:
             f.close()
     else:
@@ -389,6 +414,15 @@ def run_ours(args, dist: Dist):
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                 "traffic": None, "kernel": "k_hop (FP64, %d-real links)" % args.link_format,
                 "algorithmic_bytes_per_launch": apply_bytes / 2}
+    if args.workload == "mrhs":
+        # the dominant kernel of the batched solve: the engine's P4 phase
+        result["roofline_fp64_hop"] = roofline
+        a4 = engine_roof["bytes_per_launch"] / (engine_roof["ms_per_launch"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": round(a4, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(a4 / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                    "kernel": "k_eng_low<P4> (FP16 + norm, 18-real FP16 links, %d sources)" % w["nrhs"],
+                    "algorithmic_bytes_per_launch": engine_roof["bytes_per_launch"],
+                    "ms_per_launch": engine_roof["ms_per_launch"]}
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": unit, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",

@@ -83,6 +83,10 @@ class _RequestResult(ctypes.Structure):
                 ("latency_seconds", ctypes.c_double), ("queue_seconds", ctypes.c_double)]
 
 
+class _EngineProfile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int * 10), ("ms", ctypes.c_double * 10)]
+
+
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("cancelled", ctypes.c_uint64), ("running", ctypes.c_uint64), ("queued", ctypes.c_uint64),
@@ -108,6 +112,8 @@ _SIGNATURES = {
     "hw_context_destroy": (ctypes.c_int, [_vp]),
     "hw_context_synchronize": (ctypes.c_int, [_vp]),
     "hw_context_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "hw_engine_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "hw_engine_profile_get": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "hw_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "hw_host_free": (ctypes.c_int, [_vp]),
     "hw_lattice_create": (ctypes.c_int, [_vp, _ip, ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -266,6 +272,18 @@ class Context:
 
     def synchronize(self):
         _check(lib().hw_context_synchronize(self.handle))
+
+    ENGINE_PHASES = ("P1", "P2", "P3", "P4", "R1", "R2", "R3", "R4", "R5", "P5")
+
+    def engine_profile(self, enable: bool) -> None:
+        """Per-phase event timing of the batched engines (hw_engine_profile_enable)."""
+        _check(lib().hw_engine_profile_enable(self.handle, int(bool(enable))))
+
+    def engine_profile_get(self, precision: str = "f16") -> dict:
+        """{phase: (launches with work, summed ms)} of one engine (hw_engine_profile_get)."""
+        out = _EngineProfile()
+        _check(lib().hw_engine_profile_get(self.handle, PRECISIONS[precision], ctypes.byref(out)))
+        return {name: (out.launches[k], out.ms[k]) for k, name in enumerate(self.ENGINE_PHASES)}
 
     def stream(self) -> int:
         """The library's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

@@ -55,6 +55,8 @@ Engine::~Engine() {
     if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
     if (pinned_states_) cudaFreeHost(pinned_states_);
     if (pinned_ctl_) cudaFreeHost(pinned_ctl_);
+    for (cudaEvent_t e : prof_ev_)
+        if (e) cudaEventDestroy(e);
 }
 
 int Engine::init() {
@@ -370,7 +372,7 @@ int Engine::configure() {
     int variant = default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
     // the tensor-core variant reads the 18-real FP16 links, which exist only with full18_
-    if (variant < 0 || variant > 4 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
+    if (variant < 0 || variant > 6 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
     if (variant != grid_.variant || mask != grid_.planes_mask) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
         if (chunk_exec_) {
@@ -388,6 +390,7 @@ int Engine::launch_chunk(int iters) {
     if ((rc = ensure_partials()) != HW_OK) return rc;
     if (use_graph_ && !chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
     if ((rc = upload_tables()) != HW_OK) return rc;
+    if (ctx_->engine_profile) return launch_chunk_profiled(iters);
     if (!use_graph_) {
         set_ptrs();
         eng_enqueue_chunk_begin(ptrs_, ctx_->stream);
@@ -402,6 +405,58 @@ int Engine::launch_chunk(int iters) {
     HW_CUDA(cudaMemcpyAsync(d_ctl_.as<int>() + 3, &iters, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
     HW_CUDA(cudaGraphLaunch(chunk_exec_, ctx_->stream));
     return HW_OK;
+}
+
+// Host-loop chunk with events around every phase; synchronises after each
+// iteration to attribute its phase times (P1..P4 count when some running slot
+// had no reliable update pending, R1..R5 when some slot made one, P5 when some
+// slot was running).
+int Engine::launch_chunk_profiled(int iters) {
+    for (cudaEvent_t &e : prof_ev_)
+        if (!e) HW_CUDA(cudaEventCreate(&e));
+    set_ptrs();
+    eng_enqueue_chunk_begin(ptrs_, ctx_->stream);
+    for (int k = 0; k < iters; k++) {
+        int running = 0, inner = 0, ru_before = 0, ru_after = 0;
+        for (int j = 0; j < kEngMaxProb; j++)
+            if (slots_[j].used) {
+                running += host_states_[j].status == ENG_RUNNING;
+                inner += host_states_[j].status == ENG_RUNNING && host_states_[j].ru == 0;
+                ru_before += host_states_[j].n_ru;
+            }
+        if (running == 0) break;
+        eng_enqueue_iteration(low_, ptrs_, grid_, ctx_->stream, prof_ev_);
+        eng_enqueue_control(ptrs_, kEngMaxProb, iters, 0, 0, ctx_->stream);
+        int rc;
+        if ((rc = read_states()) != HW_OK) return rc;
+        for (int j = 0; j < kEngMaxProb; j++)
+            if (slots_[j].used) ru_after += host_states_[j].n_ru;
+        for (int ph = 0; ph < kEngPhases; ph++) {
+            const bool ru_phase = ph >= PH_R1 && ph <= PH_R5;
+            if (ru_phase && ru_after == ru_before) continue;
+            if (ph <= PH_P4 && inner == 0) continue;
+            float ms = 0.f;
+            HW_CUDA(cudaEventElapsedTime(&ms, prof_ev_[ph], prof_ev_[ph + 1]));
+            prof_ms_[ph] += ms;
+            prof_n_[ph] += 1;
+        }
+    }
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+void Engine::reset_profile() {
+    for (int ph = 0; ph < kEngPhases; ph++) {
+        prof_n_[ph] = 0;
+        prof_ms_[ph] = 0.0;
+    }
+}
+
+void Engine::profile(int *launches, double *ms) const {
+    for (int ph = 0; ph < kEngPhases; ph++) {
+        launches[ph] = (int)prof_n_[ph];
+        ms[ph] = prof_ms_[ph];
+    }
 }
 
 int Engine::read_states() {

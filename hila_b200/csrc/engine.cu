@@ -260,16 +260,17 @@ __device__ void finish(EngState &s, const EngProblem &pr, const double *tot, int
 
 // ------------------------------------------------------------------ hop phases
 
-// Arrival of one tile of lattice l; the last tile of the lattice sums every
-// active slot's partials in tile order and runs the finisher.
+// Arrival of one work item of lattice l (a tile, or a (tile, slot) pair: the
+// lattice expects `expected` of them); the last arrival sums every active
+// slot's partials in tile order and runs the finisher.
 template <int PHASE, int NRED>
 __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLattice &La, int l, double *smem,
-                                                  bool &last) {
+                                                  bool &last, int expected) {
     const EngTables *T = P.T;
     if (threadIdx.x == 0) {
         __threadfence();
         unsigned t = atomicAdd(P.tickets + l, 1u);
-        last = (t == (unsigned)La.ntiles - 1u);
+        last = (t == (unsigned)expected - 1u);
     }
     __syncthreads();
     if (last) {
@@ -361,6 +362,9 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
                     const int j = s_act[g0 + r];
                     double red[2] = {0.0, 0.0};
                     if (valid) epi_low<PHASE, LOW>(T->prob[j], P.S[j], stride, i, acc[r], red);
+                    // the block-wide sum per slot also keeps the warps of a block on the
+                    // same slot (neighbour reads shared in L1; measured faster than one
+                    // barrier per tile)
                     if constexpr (NRED > 0) {
                         double sum = block_sum<kEngTile>(red[0], smem);
                         if (threadIdx.x == 0) P.partials[((size_t)j * 2) * max_tiles + lt] = sum;
@@ -369,77 +373,73 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
             }
         }
         __syncthreads();  // s_act is rewritten by the next tile
-        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED>(P, La, l, smem, last);
+        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED>(P, La, l, smem, last, La.ntiles);
     }
 }
 
 // FP64 reliable-update phases R2..R5 for lattices whose FP64 links have PLANES
 // planes per (parity, dir); a second launch serves the other format if present.
+// Work items are (tile, a) pairs, a the position of a slot in the lattice's list
+// of slots with a pending reliable update, so each block iteration is one
+// independent hop over 128 sites (no loop over slots inside a block) and the
+// lattice's last arrival (tiles x active slots of them) runs the finisher.
+// Items of one tile are consecutive, so its links are re-read from L2.
 template <int PHASE, int LOW, int PLANES>
-__global__ void __launch_bounds__(kEngTile, 2) k_eng_f64(EngPtrs P) {
+__global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
     constexpr int SIGN = (PHASE == PH_R2 || PHASE == PH_R3) ? 1 : -1;
     constexpr int OUTPAR = (PHASE == PH_R2 || PHASE == PH_R4) ? 1 : 0;
     constexpr int NRED = (PHASE == PH_R3 || PHASE == PH_R5) ? 2 : 0;
     using Lk = typename std::conditional<PLANES == 9, LinksF64x18, LinksF64x12>::type;
     __shared__ double smem[kEngTile / 32];
     __shared__ bool last;
-    __shared__ int s_act[kEngMaxRhs];
-    __shared__ int s_na;
     if (*(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
     const EngTables *T = P.T;
-    const int ntiles = T->ntiles;
+    const int nitems = T->ntiles * kEngMaxRhs;
     const int max_tiles = T->max_tiles;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int tile = item / kEngMaxRhs, a = item % kEngMaxRhs;
         const int l = find_lattice(T, tile);
         const EngLattice &La = T->lat[l];
-        if (La.l64_planes != PLANES) continue;
-        if (threadIdx.x == 0) {
-            int na = 0;
-            for (int q = 0; q < La.nprob; q++) {
-                const int j = La.prob[q];
-                if (active<PHASE>(P.S[j])) s_act[na++] = j;
+        if (La.l64_planes != PLANES || a >= La.nprob) continue;
+        // the a-th slot with a pending update (states change only in the finisher,
+        // which runs after every item of the lattice has arrived)
+        int j = -1, na = 0;
+        for (int q = 0; q < La.nprob; q++) {
+            const int jq = La.prob[q];
+            if (active<PHASE>(P.S[jq])) {
+                if (na == a) j = jq;
+                na++;
             }
-            s_na = na;
         }
-        __syncthreads();
-        const int na = s_na;
-        if (na > 0) {
-            const Geom g = La.g;
-            const int stride = La.stride;
-            const int lt = tile - La.tile0;
-            const int i = lt * kEngTile + threadIdx.x;
-            const bool valid = i < g.Vh;
-            SiteNbrs nb;
-            if (valid) nb = site_neighbours(g, i, OUTPAR);
+        if (j < 0) continue;
+        const Geom g = La.g;
+        const int stride = La.stride;
+        const int lt = tile - La.tile0;
+        const int i = lt * kEngTile + threadIdx.x;
+        const EngProblem &pr = T->prob[j];
+        double red[2] = {0.0, 0.0};
+        if (i < g.Vh) {
+            const SiteNbrs nb = site_neighbours(g, i, OUTPAR);
             const Lk U{La.l64, stride};
-            for (int a = 0; a < na; a++) {
-                const int j = s_act[a];
-                const EngProblem &pr = T->prob[j];
-                double red[2] = {0.0, 0.0};
-                if (valid) {
-                    const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
-                    const SpinorF64 sin{const_cast<double2 *>(in), stride};
-                    Spinor<double> acc;
+            const double2 *in = (PHASE == PH_R2) ? pr.x : (PHASE == PH_R4 ? pr.s : pr.t64);
+            const SpinorF64 sin{const_cast<double2 *>(in), stride};
+            Spinor<double> acc;
 #pragma unroll
-                    for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {0.0, 0.0};
-                    // spinor first, link second: fewer values live than the multi-source hop
-                    hop_dir<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
-                    hop_dir<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
-                    hop_dir<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
-                    hop_dir<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
-                    epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
-                }
-                if constexpr (NRED > 0) {
-#pragma unroll
-                    for (int k = 0; k < NRED; k++) {
-                        double sum = block_sum<kEngTile>(red[k], smem);
-                        if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
-                    }
-                }
-            }
+            for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {0.0, 0.0};
+            hop_dir<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
         }
-        __syncthreads();  // s_act is rewritten by the next tile
-        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED>(P, La, l, smem, last);
+        if constexpr (NRED > 0) {
+#pragma unroll
+            for (int k = 0; k < NRED; k++) {
+                double sum = block_sum<kEngTile>(red[k], smem);
+                if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
+            }
+            arrive_and_finish<PHASE, NRED>(P, La, l, smem, last, La.ntiles * na);
+        }
     }
 }
 
@@ -594,34 +594,56 @@ void launch_f64(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
     if (G.planes_mask & 2) k_eng_f64<PHASE, LOW, 6><<<G.f64, kEngTile, 0, s>>>(P);
 }
 
-template <int LOW, int NR, int MINB, bool FULL18>
-void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
-    k_eng_low<PH_P1, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
-    k_eng_low<PH_P2, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
-    k_eng_low<PH_P3, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
-    k_eng_low<PH_P4, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+// profiling marks: ev (when not null) holds kEngPhases + 1 events, ev[k] recorded before phase k
+inline void mark(const cudaEvent_t *ev, int k, cudaStream_t s) {
+    if (ev) cudaEventRecord(ev[k], s);
+}
+
+// R1..R5 and P5 (phases 4..9), shared by every launch shape of the inner phases
+template <int LOW>
+void enqueue_reliable_update(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     k_eng_vec<PH_R1, LOW><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 5, s);
     launch_f64<PH_R2, LOW>(P, G, s);
+    mark(ev, 6, s);
     launch_f64<PH_R3, LOW>(P, G, s);
+    mark(ev, 7, s);
     launch_f64<PH_R4, LOW>(P, G, s);
+    mark(ev, 8, s);
     launch_f64<PH_R5, LOW>(P, G, s);
+    mark(ev, 9, s);
     k_eng_vec<PH_P5, LOW><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 10, s);
+}
+
+template <int LOW, int NR, int MINB, bool FULL18>
+void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
+    mark(ev, 0, s);
+    k_eng_low<PH_P1, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 1, s);
+    k_eng_low<PH_P2, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 2, s);
+    k_eng_low<PH_P3, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 3, s);
+    k_eng_low<PH_P4, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 4, s);
+    enqueue_reliable_update<LOW>(P, G, s, ev);
 }
 
 constexpr int kMmaMinBlocks = 4;
 
 // FP16 inner phases on the tensor cores (engine_mma.cuh), the rest as usual
-void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
+    mark(ev, 0, s);
     k_eng_mma<PH_P1, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 1, s);
     k_eng_mma<PH_P2, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 2, s);
     k_eng_mma<PH_P3, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 3, s);
     k_eng_mma<PH_P4, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
-    k_eng_vec<PH_R1, LOW_F16><<<G.low, kEngTile, 0, s>>>(P);
-    launch_f64<PH_R2, LOW_F16>(P, G, s);
-    launch_f64<PH_R3, LOW_F16>(P, G, s);
-    launch_f64<PH_R4, LOW_F16>(P, G, s);
-    launch_f64<PH_R5, LOW_F16>(P, G, s);
-    k_eng_vec<PH_P5, LOW_F16><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 4, s);
+    enqueue_reliable_update<LOW_F16>(P, G, s, ev);
 }
 
 // Launch shapes of the low-precision phases (EngGrid::variant):
@@ -630,44 +652,52 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
 //   2: one right-hand side per thread, <= 85 registers (6 blocks)
 //   3: two right-hand sides per thread sharing the links, <= 128 registers
 //   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
+//   5: one right-hand side per thread, <= 72 registers (7 blocks)
+//   6: one right-hand side per thread, <= 64 registers (8 blocks)
 // variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
 template <int LOW, bool FULL18>
-void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     if (LOW == LOW_F16 && G.variant == 4) {
-        enqueue_iteration_mma(P, G, s);
+        enqueue_iteration_mma(P, G, s, ev);
         return;
     }
     switch (G.variant) {
     case 1:
-        enqueue_iteration_t<LOW, 1, 5, FULL18>(P, G, s);
+        enqueue_iteration_t<LOW, 1, 5, FULL18>(P, G, s, ev);
         break;
     case 2:
-        enqueue_iteration_t<LOW, 1, 6, FULL18>(P, G, s);
+        enqueue_iteration_t<LOW, 1, 6, FULL18>(P, G, s, ev);
         break;
     case 3:
-        enqueue_iteration_t<LOW, 2, 4, FULL18>(P, G, s);
+        enqueue_iteration_t<LOW, 2, 4, FULL18>(P, G, s, ev);
+        break;
+    case 5:
+        enqueue_iteration_t<LOW, 1, 7, FULL18>(P, G, s, ev);
+        break;
+    case 6:
+        enqueue_iteration_t<LOW, 1, 8, FULL18>(P, G, s, ev);
         break;
     default:
-        enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s);
+        enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s, ev);
         break;
     }
 }
 
 template <int LOW>
-void enqueue_iteration_nr(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+void enqueue_iteration_nr(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     if (G.full18)
-        enqueue_iteration_v<LOW, true>(P, G, s);
+        enqueue_iteration_v<LOW, true>(P, G, s, ev);
     else
-        enqueue_iteration_v<LOW, false>(P, G, s);
+        enqueue_iteration_v<LOW, false>(P, G, s, ev);
 }
 
 }  // namespace
 
-void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     if (low == LOW_F16)
-        enqueue_iteration_nr<LOW_F16>(P, G, s);
+        enqueue_iteration_nr<LOW_F16>(P, G, s, ev);
     else
-        enqueue_iteration_nr<LOW_F32>(P, G, s);
+        enqueue_iteration_nr<LOW_F32>(P, G, s, ev);
 }
 
 void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
@@ -704,6 +734,10 @@ int occupancy_variant(int v) {
         return occupancy_low<LOW, 1, 6>();
     case 3:
         return occupancy_low<LOW, 2, 4>();
+    case 5:
+        return occupancy_low<LOW, 1, 7>();
+    case 6:
+        return occupancy_low<LOW, 1, 8>();
     default:
         return occupancy_low<LOW, 1, 4>();
     }

@@ -119,12 +119,15 @@ struct EngGrid {
 };
 
 enum EngPhase : int { PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R5, PH_P5 };
+constexpr int kEngPhases = 10;
 
 // low-precision format of one engine (template parameter of the inner phases)
 enum EngLow : int { LOW_F32 = 1, LOW_F16 = 2 };
 
-// Enqueue one CG iteration (all phases) on stream s.
-void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s);
+// Enqueue one CG iteration (all phases) on stream s.  With ev (kEngPhases + 1
+// events) ev[k] is recorded before phase k and ev[kEngPhases] after the last.
+void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s,
+                           const cudaEvent_t *ev = nullptr);
 // While-loop control: counts running slots, stops after `chunk` iterations or when none runs.
 void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
                          cudaStream_t s);

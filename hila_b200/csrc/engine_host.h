@@ -47,6 +47,10 @@ class Engine {
     int read_states();
     // loop bodies (10 phase kernels + 1 control kernel each) run since init, as of the last read_states
     unsigned long long bodies_total() const { return bodies_total_; }
+    // per-phase device time of the iterations that had work in that phase, while the
+    // context's engine profiling is on (iterations then run from a synchronising host loop)
+    void reset_profile();
+    void profile(int *launches, double *ms) const;
     const EngState &state(int slot) const { return host_states_[slot]; }
     void release(int slot);
     int nslots_used() const;
@@ -77,6 +81,10 @@ class Engine {
     EngState *pinned_states_ = nullptr;
     int *pinned_ctl_ = nullptr;
     unsigned long long bodies_total_ = 0;
+    cudaEvent_t prof_ev_[kEngPhases + 1] = {};
+    long prof_n_[kEngPhases] = {};
+    double prof_ms_[kEngPhases] = {};
+    int launch_chunk_profiled(int iters);
     DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_;
     size_t partial_tiles_ = 0;
     EngGrid grid_{};

@@ -341,8 +341,10 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_mma(EngPtrs P) {
 #pragma unroll
                 for (int w = 0; w < NW; w++) a += wsm[w].acc[threadIdx.x];
                 P.partials[((size_t)s_act[threadIdx.x] * 2) * max_tiles + lt] = a;
+                __threadfence();
             }
-            arrive_and_finish<PHASE, NRED>(P, La, l, smem, last);
+            __syncthreads();  // every partial written before thread 0 takes the ticket
+            arrive_and_finish<PHASE, NRED>(P, La, l, smem, last, La.ntiles);
         } else {
             __syncthreads();  // s_act and the warp buffers are rewritten by the next tile
         }

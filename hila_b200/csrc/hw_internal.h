@@ -78,6 +78,7 @@ struct hw_context {
     }
     size_t red_capacity_doubles = 0;
     hw::Engine *engines[3] = {nullptr, nullptr, nullptr};  // batched mixed-precision engines by precision
+    bool engine_profile = false;  // per-phase event timing of the engines (hw_engine_profile_enable)
 };
 
 // FP64 half-lattice field buffer

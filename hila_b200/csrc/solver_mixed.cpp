@@ -167,4 +167,24 @@ int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_
     return status;
 }
 
+int hw_engine_profile_enable(hw_context *ctx, int enable) {
+    HW_CHECK_ARG(ctx, "ctx is null");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (enable && !ctx->engine_profile)
+        for (Engine *e : ctx->engines)
+            if (e) e->reset_profile();
+    ctx->engine_profile = enable != 0;
+    return HW_OK;
+}
+
+int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out) {
+    HW_CHECK_ARG(ctx && out, "null argument");
+    HW_CHECK_ARG(precision == HW_PREC_F32 || precision == HW_PREC_F16, "precision must be HW_PREC_F32 or HW_PREC_F16");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    std::memset(out, 0, sizeof(*out));
+    static_assert(HW_ENGINE_PHASES == kEngPhases, "phase count");
+    if (Engine *e = ctx->engines[low_of(precision)]) e->profile(out->launches, out->ms);
+    return HW_OK;
+}
+
 }  // extern "C"

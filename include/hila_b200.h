@@ -277,6 +277,26 @@ int hw_server_wait(hw_server *server, uint64_t request_id, double *const *soluti
 int hw_server_cancel(hw_server *server, uint64_t request_id);
 int hw_server_stats_get(hw_server *server, hw_server_stats *stats);
 
+/* ------------------------------------------------------------------ profiling */
+
+/* Device time per phase of the batched mixed-precision engines behind
+ * hw_cg_solve / hw_wilson_evenodd_solve (FP32, FP16) and hw_batch_solve, from
+ * CUDA events around every phase launch (the reference has no counterpart; it
+ * times whole calls, bench_fermion.cpp:95-120).  While enabled, iterations run
+ * from a host loop that synchronises after each one, so solves are slower; the
+ * phase times are those of the same kernels.  Phases 0..9: P1 t = H p, P2
+ * Dp = M p and |Dp|^2, P3 t = H^dag Dp, P4 r -= alpha M^dag Dp, y += alpha p,
+ * |r|^2, R1..R5 the FP64 reliable update, P5 p = r + beta p. */
+#define HW_ENGINE_PHASES 10
+typedef struct hw_engine_profile {
+    int launches[HW_ENGINE_PHASES]; /* launches that had work */
+    double ms[HW_ENGINE_PHASES];    /* their summed device time */
+} hw_engine_profile;
+/* enabling resets the counters of the context's engines */
+int hw_engine_profile_enable(hw_context *ctx, int enable);
+/* counters of the engine of one precision (HW_PREC_F32 / HW_PREC_F16); zeros if it has not run */
+int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out);
+
 /* ------------------------------------------------------------------ inputs */
 
 /* Seeded synthetic inputs (no reference counterpart beyond hila::seed_random
