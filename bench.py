@@ -60,6 +60,11 @@ WORKLOADS = {
 # inputs; the CPU runs the same algorithm, so the count is the same.
 ITERS_PER_SOLVE = {"cg": 59, "mrhs": 59, "cg8": None}
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k_eng_low<P4> launch per
+# output site, 12 FP16 sources with 18-real FP16 links: 999.2 MB over 165,888 sites in one ncu
+# capture at 24^4; every array is read once, so it scales with the sites.
+P4_TRAFFIC_PER_SITE_12 = 999.2e6 / 165888
+
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -418,8 +423,12 @@ def run_ours(args, dist: Dist):
         # the dominant kernel of the batched solve: the engine's P4 phase
         result["roofline_fp64_hop"] = roofline
         a4 = engine_roof["bytes_per_launch"] / (engine_roof["ms_per_launch"] * 1e-3) / 1e9
+        traffic = None
+        if w["nrhs"] == 12 and prec == "f16":
+            traffic = {"bytes_per_launch": int(P4_TRAFFIC_PER_SITE_12 * V // 2),
+                       "source": "ncu capture at 24^4 scaled by sites"}
         roofline = {"bound": "hbm", "achieved": round(a4, 1), "peak": peak, "unit": "GB/s",
-                    "frac": round(a4 / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                    "frac": round(a4 / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
                     "kernel": "k_eng_low<P4> (FP16 + norm, 18-real FP16 links, %d sources)" % w["nrhs"],
                     "algorithmic_bytes_per_launch": engine_roof["bytes_per_launch"],
                     "ms_per_launch": engine_roof["ms_per_launch"]}
