@@ -80,49 +80,31 @@ def hbm_peak():
 # ------------------------------------------------------------------ distributed plumbing
 
 class Dist:
+    """Replica plumbing (hila_b200.replicas.ReplicaGroup), initialised by the arm that runs."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = False
+        self.group = None
 
     def init(self, backend):
-        if self.world > 1:
-            import torch.distributed as dist
-            import datetime
-            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-            self.pg = True
+        from hila_b200.replicas import ReplicaGroup
+        self.group = ReplicaGroup(backend)
 
     def barrier(self):
-        if self.pg:
-            import torch.distributed as dist
-            dist.barrier()
+        if self.group:
+            self.group.barrier()
 
     def max(self, v: float) -> float:
-        if not self.pg:
-            return v
-        import torch
-        import torch.distributed as dist
-        dev = f"cuda:{self.local_rank}" if dist.get_backend() == "nccl" else "cpu"
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return self.group.max(v) if self.group else v
 
     def sum(self, v: float) -> float:
-        if not self.pg:
-            return v
-        import torch
-        import torch.distributed as dist
-        dev = f"cuda:{self.local_rank}" if dist.get_backend() == "nccl" else "cpu"
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return self.group.sum(v) if self.group else v
 
     def close(self):
-        if self.pg:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        if self.group:
+            self.group.close()
 
 
 # ------------------------------------------------------------------ clocks
