@@ -572,12 +572,15 @@ def run_serve(args, dist: Dist):
                 "d2h_bytes_per_step": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs))},
         "latency_ms_p50": pct(lat_ms, 0.5), "latency_ms_p99": pct(lat_ms, 0.99),
         "queue_ms_p50": pct([1e3 * r.queue_seconds for r in results], 0.5),
+        "submit_lag_ms_max": round(1e3 * max(ts - (t0 + r[0]) for ts, r in zip(t_sub, reqs)), 3),
         "all_converged": ok, "max_true_residual": max(r.true_residual for r in results),
         "spot_check_residual": chk, "solves": solves, "wall_s": round(t_wall, 3),
         "fifo_f64": {"solves_per_s": round(fifo_rate, 3), "capacity_solves_per_s": round(fifo_capacity, 3),
                      "latency_ms_p50": pct(lat64, 0.5), "latency_ms_p99": pct(lat64, 0.99),
                      "all_converged": ok64},
-        "server_stats": {k: st[k] for k in ("completed", "solves_completed", "rejected", "cancelled")},
+        "server_stats": {k: (round(st[k] - st0[k], 3) if k.startswith("seconds") else st[k])
+                         for k in ("completed", "solves_completed", "rejected", "cancelled", "seconds_admit",
+                                   "seconds_run", "seconds_retire")},
         "gpu_launches": int(st["kernel_launches"] - st0["kernel_launches"]),
         "chunks": int(st["chunks"] - st0["chunks"]), "clocks": clk, "impl": "ours",
     }

@@ -26,6 +26,7 @@ class Engine {
     ~Engine();
     int init();
     int low() const { return low_; }
+    bool full18() const { return full18_; }  // inner phases read 18-real links
 
     // index of the lattice of `gauge` in this engine, adding it if needed
     int lattice_index(const hw_gauge *gauge, int *idx);

@@ -2,8 +2,9 @@
 //
 // Client threads queue requests (gauge, kappa, sources, accuracy); one server
 // thread owns the GPU work.  Every loop it
-//   1. admits queued requests in arrival order while their solve memory fits
-//      the budget and the engine has free slots on their lattice,
+//   1. admits queued requests in arrival order per lattice (a request waiting
+//      for slots on its lattice holds back later requests for that lattice
+//      only) while their solve memory fits the budget,
 //   2. runs one chunk of CG iterations for every admitted solve (one launch per
 //      phase for all of them),
 //   3. retires requests whose solves all finished and hands their solutions to
@@ -36,20 +37,82 @@ using Clock = std::chrono::steady_clock;
 
 enum ReqState { REQ_QUEUED, REQ_RUNNING, REQ_DONE };
 
+// Recycled page-locked host buffers, so source and solution copies run
+// asynchronously at full PCIe rate (page-locking memory per request would
+// cost more than the copy).
+class PinnedPool {
+  public:
+    ~PinnedPool() {
+        for (auto &e : free_) cudaFreeHost(e.second);
+    }
+    // an idle buffer of n doubles, or null (never allocates)
+    double *try_get(size_t n) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.find(n);
+        if (it == free_.end()) return nullptr;
+        double *p = it->second;
+        free_.erase(it);
+        held_ -= n;
+        return p;
+    }
+    double *get(size_t n) {
+        if (double *p = try_get(n)) return p;
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) return nullptr;
+        return static_cast<double *>(p);
+    }
+    void put(double *p, size_t n) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu_);
+        if ((held_ + n) * sizeof(double) > kKeepBytes) {
+            cudaFreeHost(p);
+            return;
+        }
+        free_.emplace(n, p);
+        held_ += n;
+    }
+
+  private:
+    static constexpr size_t kKeepBytes = size_t(4) << 30;  // idle buffers kept for reuse
+    std::mutex mu_;
+    std::multimap<size_t, double *> free_;
+    size_t held_ = 0;  // doubles in free_
+};
+
 struct Request {
     uint64_t id = 0;
     int gauge_id = 0;
     double kappa = 0, tol = 0;
     int maxiters = 0;
     int nrhs = 0;
-    std::vector<std::vector<double>> src;  // EVEN sites, checkerboard order, 24 doubles each
-    std::vector<std::vector<double>> sol;  // same layout, filled on completion
+    PinnedPool *pool = nullptr;
+    size_t n = 0;  // doubles per source / solution (EVEN sites x 24)
+    // sources, EVEN sites in checkerboard order, in pinned buffers of the pool (each
+    // later receives its solution); pageable only if page-locking fails
+    std::vector<double *> pin;
+    std::vector<std::unique_ptr<double[]>> src;
+    std::vector<double *> sol;  // pinned, same layout, filled on completion
+    const double *source(int k) const { return pin[k] ? pin[k] : src[k].get(); }
     std::vector<int> slots;
     size_t bytes = 0;
     ReqState state = REQ_QUEUED;
     bool cancel = false;
     hw_request_result res{};
     Clock::time_point t_submit, t_admit;
+    void release_sources() {  // pinned sources stay until they become solutions
+        src.clear();
+        src.shrink_to_fit();
+    }
+    void release_solutions() {
+        for (double *p : sol) pool->put(p, n);
+        sol.clear();
+        for (double *p : pin) pool->put(p, n);
+        pin.clear();
+    }
+    ~Request() {
+        release_sources();
+        release_solutions();
+    }
 };
 
 struct GaugeEntry {
@@ -91,6 +154,7 @@ void scatter_even(const GaugeEntry &G, const double *cb, double *lex) {
 
 struct hw_server {
     hw_context *ctx = nullptr;
+    hw::PinnedPool pool;  // outlives every request (declared before them)
     std::unique_ptr<hw::Engine> eng;
     hw_server_config cfg{};
     std::vector<hw::GaugeEntry> gauges;
@@ -106,20 +170,45 @@ struct hw_server {
     bool stop = false;
     std::thread worker;
     std::string worker_error;
-    hw::DevBuf stage;  // checkerboard AoS staging for one half field
     uint64_t layout_launches = 0;  // AoS <-> SoA kernels of admit / retire
+    // Host <-> device copies and layout conversions of admitted / retired solves run on
+    // their own stream, ordered against the engine's stream by events, so they overlap
+    // the chunks of the other solves.
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> free_events;
+    struct Round {
+        cudaEvent_t done;                                // solutions of `reqs` are on the host
+        std::vector<std::shared_ptr<hw::Request>> reqs;
+    };
+    std::deque<Round> retiring;
+    cudaEvent_t event() {
+        if (!free_events.empty()) {
+            cudaEvent_t e = free_events.back();
+            free_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        return e;
+    }
 };
 
 namespace hw {
 namespace {
 
-// queue -> engine slots (context lock and server lock held)
+// queue -> engine slots (context lock and server lock held).  Arrival order is
+// kept per lattice: a request without enough free slots on its lattice holds
+// back the later requests for that lattice, not those for other lattices.  A
+// request that does not fit the memory budget stops admission (the budget is
+// shared by all lattices).
 int admit_waiting(hw_server *S) {
     Engine &E = *S->eng;
-    while (!S->queue.empty()) {
-        std::shared_ptr<Request> q = S->queue.front();
+    std::vector<int> blocked;  // lattices with a waiting request ahead in the queue
+    bool admitted = false;
+    for (auto it = S->queue.begin(); it != S->queue.end();) {
+        std::shared_ptr<Request> q = *it;
         if (q->cancel) {
-            S->queue.pop_front();
+            it = S->queue.erase(it);
             q->state = REQ_DONE;
             q->res.status = HW_ERR_CANCELLED;
             q->res.nrhs = q->nrhs;
@@ -131,10 +220,18 @@ int admit_waiting(hw_server *S) {
         int l;
         int rc = E.lattice_index(G.gauge, &l);
         if (rc != HW_OK) return rc;
-        if (E.free_slots_on(l) < q->nrhs) break;  // wait for slots on this lattice (keeps arrival order)
+        if (std::find(blocked.begin(), blocked.end(), l) != blocked.end()) {
+            ++it;
+            continue;
+        }
+        if (E.free_slots_on(l) < q->nrhs) {
+            blocked.push_back(l);
+            ++it;
+            continue;
+        }
         const size_t need = (size_t)q->nrhs * E.slot_bytes(l);
-        if (S->bytes_in_use + need > S->cfg.hbm_budget_bytes) break;  // wait for memory
-        S->queue.pop_front();
+        if (S->bytes_in_use + need > S->cfg.hbm_budget_bytes) break;
+        it = S->queue.erase(it);
         q->bytes = need;
         S->bytes_in_use += need;
         q->t_admit = Clock::now();
@@ -146,25 +243,40 @@ int admit_waiting(hw_server *S) {
                               &slot)) != HW_OK)
                 return rc;
             q->slots.push_back(slot);
-            // source: host (checkerboard AoS) -> staging -> slot-owned b; x = 0
-            HW_CUDA(cudaMemcpyAsync(S->stage.ptr, q->src[k].data(), q->src[k].size() * sizeof(double),
-                                    cudaMemcpyHostToDevice, ctx->stream));
-            launch_aos_to_soa((int)G.Vh, S->stage.as<double>(), HalfF64{E.own_b(slot), stride}, ctx->stream);
+            // source: host (checkerboard AoS) -> the slot's x buffer as staging -> SoA b;
+            // then x = 0, on the copy stream (the pageable source is staged by the
+            // driver before the call returns, so it can be freed right after)
+            double *stage = reinterpret_cast<double *>(E.own_x(slot));
+            HW_CUDA(cudaMemcpyAsync(stage, q->source(k), q->n * sizeof(double), cudaMemcpyHostToDevice,
+                                    S->copy_stream));
+            launch_aos_to_soa((int)G.Vh, stage, HalfF64{E.own_b(slot), stride}, S->copy_stream);
             S->layout_launches++;
-            HW_CUDA(cudaMemsetAsync(E.own_x(slot), 0, (size_t)12 * stride * sizeof(double2), ctx->stream));
+            HW_CUDA(cudaMemsetAsync(E.own_x(slot), 0, (size_t)12 * stride * sizeof(double2), S->copy_stream));
         }
-        q->src.clear();
-        q->src.shrink_to_fit();
+        q->release_sources();
         q->state = REQ_RUNNING;
         S->running.push_back(q);
+        admitted = true;
+    }
+    if (admitted) {  // the next chunk starts after the new sources are in place
+        cudaEvent_t e = S->event();
+        HW_CUDA(cudaEventRecord(e, S->copy_stream));
+        HW_CUDA(cudaStreamWaitEvent(S->ctx->stream, e, 0));
+        S->free_events.push_back(e);
     }
     return HW_OK;
 }
 
-// finished requests -> host solutions (context lock and server lock held)
+// finished requests -> host solutions (context lock and server lock held).
+// After the engine's stream is done with them, each solution is converted to
+// checkerboard AoS in the slot's b buffer (no longer needed) and copied to a
+// pinned host buffer on the copy stream, overlapping the next chunk; the
+// round's requests complete when its event does (finish_rounds).
 int retire_finished(hw_server *S) {
     Engine &E = *S->eng;
     hw_context *ctx = S->ctx;
+    std::vector<std::shared_ptr<Request>> done;
+    bool ordered = false;
     for (size_t n = 0; n < S->running.size();) {
         std::shared_ptr<Request> q = S->running[n];
         bool all_done = true;
@@ -181,7 +293,14 @@ int retire_finished(hw_server *S) {
             status = HW_ERR_CANCELLED;
             S->stats.cancelled++;
         } else {
-            q->sol.resize(q->nrhs);
+            if (!ordered) {
+                cudaEvent_t e = S->event();
+                HW_CUDA(cudaEventRecord(e, ctx->stream));
+                HW_CUDA(cudaStreamWaitEvent(S->copy_stream, e, 0));
+                S->free_events.push_back(e);
+                ordered = true;
+            }
+            q->sol.assign(q->nrhs, nullptr);
             for (int k = 0; k < q->nrhs; k++) {
                 const int slot = q->slots[k];
                 const EngState &s = E.state(slot);
@@ -193,29 +312,66 @@ int retire_finished(hw_server *S) {
                     status = HW_ERR_BREAKDOWN;
                 else if (s.status != ENG_CONVERGED && status == HW_OK)
                     status = HW_ERR_NOT_CONVERGED;
-                q->sol[k].resize((size_t)G.Vh * 24);
+                // the pinned source buffer (its copy to the device finished earlier on this
+                // stream) receives the solution
+                q->sol[k] = q->pin[k] ? q->pin[k] : S->pool.get(q->n);
+                q->pin[k] = nullptr;
+                if (!q->sol[k]) {
+                    set_error("page-locked host allocation of %zu bytes failed", q->n * sizeof(double));
+                    return HW_ERR_OOM;
+                }
                 const int l = E.slot_lattice(slot);
-                launch_soa_to_aos((int)G.Vh, HalfF64{E.own_x(slot), E.lattice(l).stride}, S->stage.as<double>(),
-                                  ctx->stream);
+                double *stage = reinterpret_cast<double *>(E.own_b(slot));
+                launch_soa_to_aos((int)G.Vh, HalfF64{E.own_x(slot), E.lattice(l).stride}, stage, S->copy_stream);
                 S->layout_launches++;
-                HW_CUDA(cudaMemcpyAsync(q->sol[k].data(), S->stage.ptr, q->sol[k].size() * sizeof(double),
-                                        cudaMemcpyDeviceToHost, ctx->stream));
-                HW_CUDA(cudaStreamSynchronize(ctx->stream));
+                HW_CUDA(cudaMemcpyAsync(q->sol[k], stage, q->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                        S->copy_stream));
             }
             S->stats.completed++;
             S->stats.solves_completed += q->nrhs;
         }
+        // a slot's buffers are reused only by copy-stream work queued after these copies
         for (int slot : q->slots) E.release(slot);
         S->bytes_in_use -= q->bytes;
         q->res.status = status;
-        q->res.latency_seconds = std::chrono::duration<double>(Clock::now() - q->t_submit).count();
-        q->res.queue_seconds = std::chrono::duration<double>(q->t_admit - q->t_submit).count();
-        if (status == HW_OK) S->latencies.push_back(q->res.latency_seconds);
-        q->state = REQ_DONE;
+        done.push_back(q);
         S->running.erase(S->running.begin() + n);
-        S->cv_done.notify_all();
+    }
+    if (!done.empty()) {
+        hw_server::Round r;
+        r.done = S->event();
+        HW_CUDA(cudaEventRecord(r.done, S->copy_stream));
+        r.reqs = std::move(done);
+        S->retiring.push_back(std::move(r));
     }
     E.prune_lattices();
+    return HW_OK;
+}
+
+// Complete the retiring rounds whose copies have finished (server lock held);
+// with block, wait for the oldest one first.
+int finish_rounds(hw_server *S, bool block) {
+    while (!S->retiring.empty()) {
+        hw_server::Round &r = S->retiring.front();
+        if (block) {
+            HW_CUDA(cudaEventSynchronize(r.done));
+            block = false;
+        } else {
+            const cudaError_t e = cudaEventQuery(r.done);
+            if (e == cudaErrorNotReady) break;
+            HW_CUDA(e);
+        }
+        const Clock::time_point now = Clock::now();
+        for (auto &q : r.reqs) {
+            q->res.latency_seconds = std::chrono::duration<double>(now - q->t_submit).count();
+            q->res.queue_seconds = std::chrono::duration<double>(q->t_admit - q->t_submit).count();
+            if (q->res.status == HW_OK) S->latencies.push_back(q->res.latency_seconds);
+            q->state = REQ_DONE;
+        }
+        S->free_events.push_back(r.done);
+        S->retiring.pop_front();
+        S->cv_done.notify_all();
+    }
     return HW_OK;
 }
 
@@ -223,10 +379,20 @@ void fail_all(hw_server *S, int rc) {
     S->worker_error = hw_last_error();
     for (auto &q : S->running) {
         for (int slot : q->slots) S->eng->release(slot);
+        q->release_solutions();  // possibly not copied: nothing is handed out
         q->res.status = rc;
         q->state = REQ_DONE;
     }
     S->running.clear();
+    for (auto &r : S->retiring) {
+        for (auto &q : r.reqs) {
+            q->release_solutions();
+            q->res.status = rc;
+            q->state = REQ_DONE;
+        }
+        S->free_events.push_back(r.done);
+    }
+    S->retiring.clear();
     for (auto &q : S->queue) {
         q->res.status = rc;
         q->state = REQ_DONE;
@@ -241,14 +407,20 @@ void server_loop(hw_server *S) {
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->running.empty(); });
+            S->cv_work.wait(lk, [&] {
+                return S->stop || !S->queue.empty() || !S->running.empty() || !S->retiring.empty();
+            });
             if (S->stop) return;
         }
         std::lock_guard<std::recursive_mutex> glk(S->ctx->mu);
         std::unique_lock<std::mutex> lk(S->mu);
         if (S->stop) return;
+        auto since = [](Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); };
+        Clock::time_point t0 = Clock::now();
         int rc = admit_waiting(S);
+        S->stats.seconds_admit += since(t0);
         if (rc == HW_OK && !S->running.empty()) {
+            t0 = Clock::now();
             rc = S->eng->launch_chunk(S->cfg.chunk_iters);
             if (rc == HW_OK) {
                 // clients can submit and wait while the chunk runs on the device
@@ -259,8 +431,13 @@ void server_loop(hw_server *S) {
                 S->stats.chunks++;
                 S->stats.kernel_launches = S->layout_launches + S->stats.chunks + 11 * S->eng->bodies_total();
             }
+            S->stats.seconds_run += since(t0);
         }
+        t0 = Clock::now();
         if (rc == HW_OK) rc = retire_finished(S);
+        // with nothing left on the engine, wait for the oldest copies instead of spinning
+        if (rc == HW_OK) rc = finish_rounds(S, S->running.empty() && S->queue.empty());
+        S->stats.seconds_retire += since(t0);
         if (rc != HW_OK) fail_all(S, rc);
     }
 }
@@ -294,6 +471,7 @@ int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server 
     S->eng.reset(new Engine(ctx, cfg.precision == HW_PREC_F16 ? LOW_F16 : LOW_F32));
     int rc = S->eng->init();
     if (rc != HW_OK) return rc;
+    HW_CUDA(cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking));
     S->stats.bytes_budget = cfg.hbm_budget_bytes;
     hw_server *raw = S.get();
     S->worker = std::thread([raw] { server_loop(raw); });
@@ -311,8 +489,13 @@ int hw_server_destroy(hw_server *S) {
     if (S->worker.joinable()) S->worker.join();
     {
         std::lock_guard<std::recursive_mutex> glk(S->ctx->mu);
+        if (S->copy_stream) cudaStreamSynchronize(S->copy_stream);
         S->eng.reset();
-        S->stage.release();
+        for (auto &r : S->retiring) S->free_events.push_back(r.done);
+        S->retiring.clear();
+        for (cudaEvent_t e : S->free_events) cudaEventDestroy(e);
+        S->free_events.clear();
+        if (S->copy_stream) cudaStreamDestroy(S->copy_stream);
     }
     delete S;
     return HW_OK;
@@ -328,13 +511,7 @@ int hw_server_add_gauge(hw_server *S, const hw_gauge *gauge, int *gauge_id) {
     G.Vh = gauge->lat->Vh;
     std::lock_guard<std::recursive_mutex> glk(S->ctx->mu);
     std::lock_guard<std::mutex> lk(S->mu);
-    const size_t need = (size_t)G.Vh * 24 * sizeof(double);
-    if (S->stage.bytes < need) {
-        HW_CUDA(cudaStreamSynchronize(S->ctx->stream));
-        int rc = S->stage.alloc(need);
-        if (rc != HW_OK) return rc;
-    }
-    int rc = ensure_low_links(gauge, S->eng->low(), false);
+    int rc = ensure_low_links(gauge, S->eng->low(), S->eng->full18());
     if (rc != HW_OK) return rc;
     tune_hop(gauge->lat, gauge);
     S->gauges.push_back(G);
@@ -365,10 +542,17 @@ int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const d
     q->maxiters = maxiters;
     q->nrhs = nrhs;
     q->t_submit = Clock::now();
+    q->pool = &S->pool;
+    q->n = (size_t)G.Vh * 24;
+    q->pin.assign(nrhs, nullptr);
     q->src.resize(nrhs);
     for (int k = 0; k < nrhs; k++) {
-        q->src[k].resize((size_t)G.Vh * 24);
-        gather_even(G, sources[k], q->src[k].data());
+        double *dst = q->pin[k] = S->pool.get(q->n);
+        if (!dst) {
+            q->src[k].reset(new double[q->n]);
+            dst = q->src[k].get();
+        }
+        gather_even(G, sources[k], dst);
     }
     std::lock_guard<std::mutex> lk(S->mu);
     q->id = S->next_id++;
@@ -378,7 +562,7 @@ int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const d
     // a request that can never fit the budget is rejected now
     const size_t need = (size_t)nrhs * S->eng->slot_bytes_for_stride(padded_stride(G.Vh));
     if (need > S->cfg.hbm_budget_bytes) {
-        q->src.clear();
+        q->release_sources();
         q->state = REQ_DONE;
         q->res.status = HW_ERR_REJECTED;
         q->res.nrhs = nrhs;
@@ -410,7 +594,7 @@ int hw_server_wait(hw_server *S, uint64_t request_id, double *const *solutions, 
     lk.unlock();
     if (solutions && !q->sol.empty())
         for (int k = 0; k < q->nrhs; k++)
-            if (solutions[k]) scatter_even(G, q->sol[k].data(), solutions[k]);
+            if (solutions[k]) scatter_even(G, q->sol[k], solutions[k]);
     return q->res.status == HW_ERR_CANCELLED || q->res.status == HW_ERR_REJECTED ? q->res.status : HW_OK;
 }
 

@@ -257,6 +257,9 @@ typedef struct hw_server_stats {
     uint64_t solves_completed;                         /* sources, not requests */
     uint64_t chunks;                                   /* chunk graphs launched */
     uint64_t kernel_launches;                          /* kernels those chunks ran */
+    double seconds_admit;                              /* server-thread wall time admitting requests */
+    double seconds_run;                                /* ... launching chunks and reading slot states */
+    double seconds_retire;                             /* ... copying solutions out and retiring */
 } hw_server_stats;
 
 int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server **server);
