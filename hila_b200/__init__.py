@@ -129,6 +129,10 @@ _SIGNATURES = {
     "hw_field_zero": (ctypes.c_int, [_vp, ctypes.c_int]),
     "hw_wilson_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_wilson_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "hw_wilson_evenodd_force": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, _dp]),
+    "hw_gauge_config_dims": (ctypes.c_int, [ctypes.c_char_p, _ip]),
+    "hw_gauge_config_write": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
+    "hw_gauge_config_read": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
     "hw_wilson_apply": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
     "hw_wilson_hop": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "hw_cg_params_default": (None, [ctypes.POINTER(_CgParams)]),
@@ -419,6 +423,13 @@ class Dirac_Wilson_evenodd:
     def dagger(self, inp: Field, out: Field):
         _check(lib().hw_wilson_evenodd_dagger(self.gauge.handle, self.kappa, inp.handle, out.handle))
 
+    def force(self, chi: Field, psi: Field, sign: int = 1) -> np.ndarray:
+        """d Re(chi^dag M_s psi) / d links (wilson.h:293-311), shape (4, V, 3, 3, 2)."""
+        out = np.zeros((4, self.gauge.lattice.volume, 3, 3, 2), np.float64)
+        _check(lib().hw_wilson_evenodd_force(self.gauge.handle, self.kappa, chi.handle, psi.handle, int(sign),
+                                             _dptr(out)))
+        return out
+
     def hop(self, inp: Field, out: Field, parity: int, sign: int, set_: bool = True):
         """Dirac_Wilson_hop_set (set_) / Dirac_Wilson_hop with this operator's kappa."""
         _check(lib().hw_wilson_hop(self.gauge.handle, self.kappa, inp.handle, out.handle, int(parity), int(sign),
@@ -574,6 +585,33 @@ class RequestResult:
     @property
     def converged(self) -> bool:
         return self.status == HW_OK
+
+
+# ------------------------------------------------------------------ configuration files
+
+def config_dims(path: str) -> tuple:
+    """Lattice size recorded in a HILA gauge configuration file (hw_gauge_config_dims)."""
+    d = (ctypes.c_int * 4)()
+    _check(lib().hw_gauge_config_dims(os.fsencode(path), d))
+    return tuple(d)
+
+
+def config_write(path: str, dims, links: np.ndarray) -> None:
+    """GaugeField::config_write (gaugefield.h:196-217): links (4, V, 3, 3, 2) to a file."""
+    links = np.ascontiguousarray(links, np.float64)
+    dims = tuple(int(v) for v in dims)
+    if links.size != 4 * int(np.prod(dims)) * 18:
+        raise ValueError("links must hold 4*V*18 doubles")
+    _check(lib().hw_gauge_config_write(os.fsencode(path), (ctypes.c_int * 4)(*dims), _dptr(links)))
+
+
+def config_read(path: str, dims=None) -> np.ndarray:
+    """GaugeField::config_read (gaugefield.h:219-271): links (4, V, 3, 3, 2) for a lattice of
+    size dims (default: the file's); a smaller file is replicated periodically."""
+    dims = tuple(int(v) for v in (dims if dims is not None else config_dims(path)))
+    out = np.zeros((4, int(np.prod(dims)), 3, 3, 2), np.float64)
+    _check(lib().hw_gauge_config_read(os.fsencode(path), (ctypes.c_int * 4)(*dims), _dptr(out)))
+    return out
 
 
 class Server:

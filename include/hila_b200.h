@@ -102,6 +102,17 @@ int hw_lattice_volume(const hw_lattice *lat, int64_t *volume);
 int hw_gauge_create(hw_lattice *lat, const double *links, int link_format, hw_gauge **gauge);
 int hw_gauge_destroy(hw_gauge *gauge);
 
+/* Gauge configuration files in HILA's binary format, GaugeField::config_write /
+ * config_read (gaugefield.h:196-271, Field::write / read field_io.h:128-330):
+ * int64 header {394824242, 4, 144, Lx, Ly, Lz, Lt}, then the links in the host
+ * layout double[4][V][3][3][2].  config_read fills a lattice whose dimensions
+ * are multiples of the file's by periodic replication; errors (wrong id,
+ * dimensionality, element size, dimensions, short file) return HW_ERR_INVALID
+ * with the reference's message in hw_last_error().  Host only. */
+int hw_gauge_config_dims(const char *path, int dims[4]);
+int hw_gauge_config_write(const char *path, const int dims[4], const double *links);
+int hw_gauge_config_read(const char *path, const int dims[4], double *links);
+
 /* FP64 Wilson spinor field, Field<Wilson_vector<3,double>> (full lattice,
  * device resident, even-odd structure-of-arrays inside). */
 int hw_field_create(hw_lattice *lat, hw_field **field);
@@ -119,6 +130,15 @@ int hw_field_zero(hw_field *field, int parity);
 int hw_wilson_evenodd_apply(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out);
 /* Dirac_Wilson_evenodd::dagger(in, out), wilson.h:282-289 (sign -1) */
 int hw_wilson_evenodd_dagger(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out);
+
+/* Dirac_Wilson_evenodd::force(chi, psi, force, sign), wilson.h:293-311 (with
+ * Dirac_Wilson_calc_force, wilson.h:110-137): the derivative of
+ * Re(chi^dag M_s psi) (chi, psi on EVEN) with respect to every link, as 3x3
+ * complex matrices in the host link layout double[4][V][3][3][2] (the HMC adds
+ * project_antihermitean(U F) to the momentum, gauge_field.h:249-256).  sign +1
+ * for M (apply), -1 for M^dag.  Synchronises. */
+int hw_wilson_evenodd_force(const hw_gauge *gauge, double kappa, const hw_field *chi, const hw_field *psi, int sign,
+                            double *force);
 
 /* Dirac_Wilson<SU<3,double>>::apply / dagger, wilson.h:183-192:
  * out = in - kappa H_s in over ALL sites (sign +1 apply, -1 dagger). */

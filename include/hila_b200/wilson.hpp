@@ -157,6 +157,15 @@ class GaugeField {
             for (int i = 0; i < 3; i++)
                 for (int j = 0; j < 3; j++) u.e[i][j] = (i == j) ? 1.0 : 0.0;
     }
+    // GaugeField::config_write / config_read (gaugefield.h:196-271), HILA's binary format
+    void config_write(const std::string &filename) const {
+        check(hw_gauge_config_write(filename.c_str(), lat_->size().data(),
+                                    reinterpret_cast<const double *>(links_.data())));
+    }
+    void config_read(const std::string &filename) {
+        invalidate();
+        check(hw_gauge_config_read(filename.c_str(), lat_->size().data(), reinterpret_cast<double *>(links_.data())));
+    }
     hw_gauge *handle() {
         if (!g_) check(hw_gauge_create(lat_->handle(), reinterpret_cast<const double *>(links_.data()), fmt_, &g_));
         return g_;
@@ -198,6 +207,17 @@ class Dirac_Wilson_evenodd {
         out.push();
         check(hw_wilson_evenodd_dagger(U_->handle(), kappa, in.handle(), out.handle()));
         out.mark_device_changed();
+    }
+    // force(chi, psi, force, sign), wilson.h:293-311: force[dir][site] = dS/dU_dir(site)
+    // of S = Re(chi^dag M_s psi), lexicographic sites
+    void force(Field<vector_type> &chi, Field<vector_type> &psi, std::vector<SU<3, double>> (&force)[4], int sign) {
+        chi.push();
+        psi.push();
+        const int64_t V = U_->lattice().volume();
+        std::vector<SU<3, double>> all((size_t)(4 * V));
+        check(hw_wilson_evenodd_force(U_->handle(), kappa, chi.handle(), psi.handle(), sign,
+                                      reinterpret_cast<double *>(all.data())));
+        for (int d = 0; d < 4; d++) force[d].assign(all.begin() + d * V, all.begin() + (d + 1) * V);
     }
     GaugeField &gauge() { return *U_; }
 

@@ -56,6 +56,7 @@ def lib():
                                   ctypes.c_int, ctypes.c_int, ctypes.c_int]),
             "or_wilson_apply": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int]),
             "or_wilson_eo_apply": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int]),
+            "or_wilson_eo_force": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int, _dp]),
             "or_dot": (v, [_ip, _dp, _dp, ctypes.c_int, _dp, _dp]),
             "or_squarenorm": (ctypes.c_double, [_ip, _dp, ctypes.c_int]),
             "or_cg": (ctypes.c_int, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp,
@@ -147,6 +148,16 @@ def cg(dims, U, kappa, inp, out=None, acc=1e-12, maxiters=10000, antiperiodic=Tr
     it = lib().or_cg(_dims(dims), int(antiperiodic), _d(U), kappa, _d(inp), _d(out), acc, maxiters,
                      ctypes.byref(rr))
     return out, it, rr.value
+
+
+def eo_force(dims, U, kappa, chi, psi, sign=1, antiperiodic=True) -> np.ndarray:
+    """Dirac_Wilson_evenodd::force (wilson.h:293-311): d Re(chi^dag M_s psi) / d links,
+    as [4][V][3][3] complex (shape (4, V, 3, 3, 2))."""
+    chi = np.ascontiguousarray(chi, np.float64)
+    psi = np.ascontiguousarray(psi, np.float64)
+    out = np.zeros((4, volume(dims), 3, 3, 2))
+    lib().or_wilson_eo_force(_dims(dims), int(antiperiodic), _d(U), kappa, _d(chi), _d(psi), sign, _d(out))
+    return out
 
 
 def true_residual(dims, U, kappa, b, x, sign=1, antiperiodic=True) -> float:

@@ -525,6 +525,56 @@ void or_wilson_eo_apply(const int *dims, int tap, const double *U, double kappa,
         if (g.in(x, 2)) std::memset(out + 24 * x, 0, 24 * sizeof(double));
 }
 
+// Dirac_Wilson_calc_force, wilson.h:110-137, accumulated into out (the caller
+// zeroes it): for every positive direction dir and site X
+//   X in par:      out[dir][X] += -k (E_{dir,-s} P_{dir,-s} chi(X+dir)) (x) psi(X)
+//   X in opp(par): out[dir][X] += -k (E_{dir,s} P_{dir,s} psi(X+dir)) (x) chi(X)
+// with (a (x) b)_ij = sum_spin a_i conj(b_j) (Matrix::outer_product, matrix.h:1437-1448,
+// summed over spin, wilson_vector.h:229-233) and the fermion boundary sign on X+dir.
+static void calc_force(const Geom &g, double k, const double *chi, const double *psi, int par, int sign,
+                       double *out) {
+    const int opp = par == 1 ? 2 : 1;
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        const bool in_par = g.in(x, par);
+        if (!in_par && !g.in(x, opp)) continue;
+        for (int dir = 0; dir < 4; dir++) {
+            double sg;
+            const long y = g.nb(x, dir, +1, &sg);
+            const int s = in_par ? -sign : sign;
+            const Spinor a = expand(project(load_spinor(in_par ? chi : psi, y), dir, s), dir, s);
+            const Spinor b = load_spinor(in_par ? psi : chi, x);
+            double *o = out + 18 * (dir * g.V + x);
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    cd acc = 0;
+                    for (int sp = 0; sp < 4; sp++) acc += a.s[sp][i] * std::conj(b.s[sp][j]);
+                    acc *= -k * sg;
+                    o[(i * 3 + j) * 2] += acc.real();
+                    o[(i * 3 + j) * 2 + 1] += acc.imag();
+                }
+        }
+    }
+}
+
+// Dirac_Wilson_evenodd::force(chi, psi, force, sign), wilson.h:293-311: the
+// derivative of Re(chi^dag M_s psi) (chi, psi on EVEN) with respect to the
+// links, as 3x3 complex matrices out[4][V][3][3] (HMC adds
+// project_antihermitean(U F) to the momentum, gauge_field.h:249-256).
+void or_wilson_eo_force(const int *dims, int tap, const double *U, double kappa, const double *chi,
+                        const double *psi, int sign, double *out) {
+    Geom g(dims, tap);
+    std::memset(out, 0, sizeof(double) * 72 * g.V);
+    std::vector<double> tmp((size_t)24 * g.V, 0.0);
+    // tmp = hop_set(kappa, chi, ODD, -sign); calc_force(-kappa, tmp, psi, EVEN, sign)
+    or_wilson_hop(dims, tap, U, kappa, chi, tmp.data(), 2, -sign, 1);
+    calc_force(g, -kappa, tmp.data(), psi, 1, sign, out);
+    // tmp = hop_set(kappa, psi, ODD, sign); calc_force(-kappa, chi, tmp, ODD, sign)
+    std::fill(tmp.begin(), tmp.end(), 0.0);
+    or_wilson_hop(dims, tap, U, kappa, psi, tmp.data(), 2, sign, 1);
+    calc_force(g, -kappa, chi, tmp.data(), 2, sign, out);
+}
+
 // sum over sites of parity par of conj(a) . b  (WilsonVector::dot, conj-linear in a)
 void or_dot(const int *dims, const double *a, const double *b, int par, double *re, double *im) {
     Geom g(dims, 0);
