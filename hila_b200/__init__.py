@@ -63,7 +63,8 @@ class HilaError(RuntimeError):
 
 class _CgParams(ctypes.Structure):
     _fields_ = [("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int), ("precision", ctypes.c_int),
-                ("delta", ctypes.c_double), ("true_residual", ctypes.c_int), ("use_graph", ctypes.c_int)]
+                ("delta", ctypes.c_double), ("true_residual", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("hasenbusch_mh", ctypes.c_double)]
 
 
 class _CgResult(ctypes.Structure):
@@ -99,7 +100,8 @@ class _ServerStats(ctypes.Structure):
 
 class _SolveRequest(ctypes.Structure):
     _fields_ = [("gauge", ctypes.c_void_p), ("kappa", ctypes.c_double), ("b", ctypes.c_void_p),
-                ("x", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int)]
+                ("x", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int),
+                ("hasenbusch_mh", ctypes.c_double)]
 
 
 _vp = ctypes.c_void_p
@@ -130,6 +132,10 @@ _SIGNATURES = {
     "hw_wilson_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_wilson_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_wilson_evenodd_force": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, _dp]),
+    "hw_hasenbusch_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    "hw_hasenbusch_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    "hw_mre_guess": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(_vp), ctypes.c_int, _vp,
+                                    _vp]),
     "hw_gauge_config_dims": (ctypes.c_int, [ctypes.c_char_p, _ip]),
     "hw_gauge_config_write": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
     "hw_gauge_config_read": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
@@ -458,6 +464,46 @@ class Dirac_Wilson_evenodd:
         return CGResult.from_c(r)
 
 
+class Hasenbusch_operator:
+    """Hasenbusch_operator<Dirac_Wilson_evenodd> (Hasenbusch.h:16-52): M + m_h on EVEN."""
+
+    def __init__(self, D: "Dirac_Wilson_evenodd", h_parameter: float):
+        self.D = D
+        self.h_parameter = float(h_parameter)
+        self.par = D.par
+
+    def apply(self, inp: Field, out: Field):
+        _check(lib().hw_hasenbusch_evenodd_apply(self.D.gauge.handle, self.D.kappa, self.h_parameter, inp.handle,
+                                                 out.handle))
+
+    def dagger(self, inp: Field, out: Field):
+        _check(lib().hw_hasenbusch_evenodd_dagger(self.D.gauge.handle, self.D.kappa, self.h_parameter, inp.handle,
+                                                  out.handle))
+
+    def force(self, chi: Field, psi: Field, sign: int = 1) -> np.ndarray:
+        """The operator's force (Hasenbusch.h:49-52): m_h does not depend on the links."""
+        return self.D.force(chi, psi, sign)
+
+    def solve(self, b: Field, x: Field, accuracy: float = 1e-10, maxiters: int = 10000, precision: str = "f64",
+              delta: float = 0.1, use_graph: bool = True) -> "CGResult":
+        """(M + m_h) x = b by CG on the normal equations."""
+        p = _params(accuracy, maxiters, precision, delta, True, use_graph, self.h_parameter)
+        r = _CgResult()
+        rc = lib().hw_wilson_evenodd_solve(self.D.gauge.handle, self.D.kappa, b.handle, x.handle, ctypes.byref(p),
+                                           ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        return CGResult.from_c(r)
+
+
+def mre_guess(op, old, chi: Field, psi: Field) -> None:
+    """MRE_guess (MRE_guess.h:9-88): psi = initial guess for op^dag op psi = chi from the
+    earlier solutions `old` (list of Field); op is Dirac_Wilson_evenodd or Hasenbusch_operator."""
+    D, mh = (op.D, op.h_parameter) if isinstance(op, Hasenbusch_operator) else (op, 0.0)
+    arr = (_vp * max(len(old), 1))(*[f.handle for f in old])
+    _check(lib().hw_mre_guess(D.gauge.handle, D.kappa, mh, arr, len(old), chi.handle, psi.handle))
+
+
 class Dirac_Wilson:
     """Dirac_Wilson<SU<3,double>> (wilson.h:146-201): D = 1 - kappa H over ALL sites."""
 
@@ -495,9 +541,10 @@ class CGResult:
                    r.seconds, r.kernel_launches)
 
 
-def _params(accuracy, maxiters, precision, delta, true_residual, use_graph) -> _CgParams:
+def _params(accuracy, maxiters, precision, delta, true_residual, use_graph, mh=0.0) -> _CgParams:
     p = _CgParams()
     lib().hw_cg_params_default(ctypes.byref(p))
+    p.hasenbusch_mh = float(mh)
     p.accuracy = float(accuracy)
     p.maxiters = int(maxiters)
     p.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
@@ -540,7 +587,8 @@ class CG:
 
 
 def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0.1) -> list:
-    """Solve many M x = b at once: requests are (op, b_field, x_field[, accuracy[, maxiters]]).
+    """Solve many M x = b at once: requests are (op, b_field, x_field[, accuracy[, maxiters]]);
+    op is a Dirac_Wilson_evenodd or a Hasenbusch_operator ((M + m_h) x = b).
 
     All right-hand sides on all lattices advance together, one kernel launch
     per CG phase (hw_batch_solve); returns one CGResult per request.
@@ -551,7 +599,9 @@ def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0
         op, b, x = req[0], req[1], req[2]
         acc = req[3] if len(req) > 3 else 1e-10
         mi = req[4] if len(req) > 4 else 10000
-        arr[k] = _SolveRequest(op.gauge.handle.value, op.kappa, b.handle.value, x.handle.value, float(acc), int(mi))
+        D, mh = (op.D, op.h_parameter) if isinstance(op, Hasenbusch_operator) else (op, 0.0)
+        arr[k] = _SolveRequest(D.gauge.handle.value, D.kappa, b.handle.value, x.handle.value, float(acc), int(mi),
+                               float(mh))
     res = (_CgResult * max(n, 1))()
     rc = lib().hw_batch_solve(ctx.handle, PRECISIONS[precision], float(delta), arr, n, res)
     if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):

@@ -1,6 +1,8 @@
 // C-ABI entry points: contexts, lattices, fields and the FP64 operators.
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include <cstdlib>
 #include <cstring>
 
@@ -343,7 +345,9 @@ static int check_op(const hw_gauge *g, const hw_field *in, const hw_field *out) 
     return HW_OK;
 }
 
-static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_field *out, int sign) {
+// out_e = d in_e - kappa^2 H^{eo}_s H^{oe}_s in_e, d = 1 + m_h (d = 1: wilson.h:272-289;
+// m_h > 0: Hasenbusch_operator::apply / dagger, Hasenbusch.h:39-47)
+static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_field *out, int sign, double d = 1.0) {
     int rc = check_op(G, in, out);
     if (rc != HW_OK) return rc;
     hw_lattice *lat = G->lat;
@@ -356,7 +360,7 @@ static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_fiel
     // t_o = H^{oe}_s in_e ; out_e = in_e - kappa^2 H^{eo}_s t_o ; out_o = 0  (wilson.h:272-279)
     launch_hop_scale(lat->g, G->U(), 1, sign, in->half[0].h(), w.t.h(), 1.0, nullptr, ctx->stream);
     launch_hop_xpay(lat->g, G->U(), 0, sign, w.t.h(), in->half[0].h(), out->half[0].h(), -kappa * kappa, nullptr,
-                    nullptr, ctx->stream);
+                    nullptr, ctx->stream, d);
     HW_CUDA(cudaMemsetAsync(out->half[1].buf.ptr, 0, out->half[1].buf.bytes, ctx->stream));
     // stream-ordered: later calls on this context see the result; downloads synchronise
     HW_CUDA(cudaGetLastError());
@@ -369,6 +373,16 @@ int hw_wilson_evenodd_apply(const hw_gauge *gauge, double kappa, const hw_field 
 
 int hw_wilson_evenodd_dagger(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out) {
     return eo_apply(gauge, kappa, in, out, -1);
+}
+
+int hw_hasenbusch_evenodd_apply(const hw_gauge *gauge, double kappa, double mh, const hw_field *in, hw_field *out) {
+    HW_CHECK_ARG(std::isfinite(mh), "mh must be finite");
+    return eo_apply(gauge, kappa, in, out, +1, 1.0 + mh);
+}
+
+int hw_hasenbusch_evenodd_dagger(const hw_gauge *gauge, double kappa, double mh, const hw_field *in, hw_field *out) {
+    HW_CHECK_ARG(std::isfinite(mh), "mh must be finite");
+    return eo_apply(gauge, kappa, in, out, -1, 1.0 + mh);
 }
 
 int hw_wilson_apply(const hw_gauge *G, double kappa, int sign, const hw_field *in, hw_field *out) {
@@ -458,3 +472,14 @@ int hw_wilson_evenodd_solve_host(const hw_gauge *G, double kappa, const double *
 }
 
 }  // extern "C"
+
+namespace hw {
+// (M_s + m_h) on EVEN half fields, stream-ordered, through the lattice's ODD
+// workspace field (context lock held; workspace and hop shape ready)
+void eo_apply_half(const hw_gauge *G, double kappa, HalfF64 in, HalfF64 out, int sign, double d) {
+    hw_lattice *lat = G->lat;
+    CgWorkspace &w = *lat->ws;
+    launch_hop_scale(lat->g, G->U(), 1, sign, in, w.t.h(), 1.0, nullptr, lat->ctx->stream);
+    launch_hop_xpay(lat->g, G->U(), 0, sign, w.t.h(), in, out, -kappa * kappa, nullptr, nullptr, lat->ctx->stream, d);
+}
+}  // namespace hw

@@ -43,19 +43,24 @@ __device__ __forceinline__ void store_c(const SpinorF64 &f, int c, int i, Cx<dou
     f.p[(size_t)c * f.stride + i] = make_double2(v.re, v.im);
 }
 
-// out = x + b * H in ; optionally pAp = |out|^2 and alpha = rr / pAp
+// d x as an uncontracted product: with d = 1 the sums below round exactly as x + b H in
+__device__ __forceinline__ Cx<double> dscale(double d, Cx<double> v) { return {__dmul_rn(d, v.re), __dmul_rn(d, v.im)}; }
+
+// out = d x + b * H in ; optionally pAp = |out|^2 and alpha = rr / pAp.  d = 1 + m_h
+// gives the Hasenbusch operator M + m_h (Hasenbusch.h:16-52), d = 1 the plain one.
 template <bool RED>
 struct EpiXpay {
     static constexpr int NRED = RED ? 1 : 0;
     SpinorF64 x, out;
     double b;
     CgState *st;
+    double d;
     __device__ bool skip() const { return st && st->status != CG_RUNNING; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> v = load_c(x, c, i) + b * acc.s[c / 3][c % 3];
+            Cx<double> v = dscale(d, load_c(x, c, i)) + b * acc.s[c / 3][c % 3];
             store_c(out, c, i, v);
             n2 += norm2(v);
         }
@@ -73,19 +78,20 @@ struct EpiXpay {
 };
 
 // CG step fused into the second hop of M^dagger (conjugate_gradient.h:77-95):
-// DDp = Dp + b H t ; x += alpha p ; r -= alpha DDp ; rrnew = |r|^2
+// DDp = d Dp + b H t ; x += alpha p ; r -= alpha DDp ; rrnew = |r|^2
 struct EpiCgUpdate {
     static constexpr int NRED = 1;
     SpinorF64 Dp, r, x, p;
     double b;
     CgState *st;
+    double d;
     __device__ bool skip() const { return st->status != CG_RUNNING; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
         const double alpha = st->alpha;
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> ddp = load_c(Dp, c, i) + b * acc.s[c / 3][c % 3];
+            Cx<double> ddp = dscale(d, load_c(Dp, c, i)) + b * acc.s[c / 3][c % 3];
             Cx<double> rv = load_c(r, c, i) - alpha * ddp;
             store_c(r, c, i, rv);
             store_c(x, c, i, load_c(x, c, i) + alpha * load_c(p, c, i));
@@ -110,19 +116,20 @@ struct EpiCgUpdate {
     }
 };
 
-// res = src - (x + b H t) ; |res|^2, |src|^2
+// res = src - (d x + b H t) ; |res|^2, |src|^2
 struct EpiResidual {
     static constexpr int NRED = 2;
     SpinorF64 x, src, res;
     double b;
     CgState *st;
+    double d;
     __device__ bool skip() const { return false; }
     __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
         double n2 = 0, d2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
             Cx<double> sv = load_c(src, c, i);
-            Cx<double> v = sv - (load_c(x, c, i) + b * acc.s[c / 3][c % 3]);
+            Cx<double> v = sv - (dscale(d, load_c(x, c, i)) + b * acc.s[c / 3][c % 3]);
             if (res.p) store_c(res, c, i, v);
             n2 += norm2(v);
             d2 += norm2(sv);
@@ -352,26 +359,26 @@ void launch_hop_scale(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF
 }
 
 void launch_hop_xpay(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 x, HalfF64 out,
-                     double b, CgState *st, const RedBuf *red, cudaStream_t s) {
+                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d) {
     if (red) {
-        EpiXpay<true> e{sp(x), sp(out), b, st};
+        EpiXpay<true> e{sp(x), sp(out), b, st, d};
         dispatch_hop(g, U, par, sign, in, e, red, s);
     } else {
-        EpiXpay<false> e{sp(x), sp(out), b, st};
+        EpiXpay<false> e{sp(x), sp(out), b, st, d};
         dispatch_hop(g, U, par, sign, in, e, nullptr, s);
     }
 }
 
 void launch_hop_cg_update(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 Dp, HalfF64 r,
                           HalfF64 x, HalfF64 p, double b, CgState *st, const RedBuf &red,
-                          cudaStream_t s) {
-    EpiCgUpdate e{sp(Dp), sp(r), sp(x), sp(p), b, st};
+                          cudaStream_t s, double d) {
+    EpiCgUpdate e{sp(Dp), sp(r), sp(x), sp(p), b, st, d};
     dispatch_hop(g, U, par, sign, t, e, &red, s);
 }
 
 void launch_hop_residual(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 x, HalfF64 src,
-                         HalfF64 res, double b, CgState *st, const RedBuf &red, cudaStream_t s) {
-    EpiResidual e{sp(x), sp(src), sp(res), b, st};
+                         HalfF64 res, double b, CgState *st, const RedBuf &red, cudaStream_t s, double d) {
+    EpiResidual e{sp(x), sp(src), sp(res), b, st, d};
     dispatch_hop(g, U, par, sign, t, e, &red, s);
 }
 

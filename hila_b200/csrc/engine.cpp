@@ -235,7 +235,7 @@ int Engine::ensure_own(int slot) {
 }
 
 int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int maxiter, double delta, int mode,
-                  int *slot_out) {
+                  int *slot_out, double diag) {
     HW_CHECK_ARG(lat >= 0 && lat < tables_.nlat, "bad lattice index");
     EngLattice &L = tables_.lat[lat];
     HW_CHECK_ARG(L.nprob < kEngMaxRhs, "lattice holds %d solves already", kEngMaxRhs);
@@ -259,6 +259,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     P.lat = lat;
     P.mode = mode;
     P.kappa = kappa;
+    P.diag = diag;
     P.p = B.p.ptr;
     P.r = B.r.ptr;
     P.Dp = B.Dp.ptr;

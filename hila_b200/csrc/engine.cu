@@ -90,6 +90,9 @@ template <int PHASE, int LOW>
 __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st, int stride, int i,
                                         Spinor<float> &acc, double *red) {
     using L = Low<LOW>;
+    // d p as an uncontracted product: with d = 1 the sums round exactly as p - k^2 acc
+    const float dg = (float)pr.diag;
+    auto ds = [dg](Cx<float> v) -> Cx<float> { return {__fmul_rn(dg, v.re), __fmul_rn(dg, v.im)}; };
     if (PHASE == PH_P1 || PHASE == PH_P3) {
         L::sp(pr.t, pr.tn, stride).store(i, acc);
     } else if (PHASE == PH_P2) {
@@ -99,7 +102,7 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<float> v = p.s[c / 3][c % 3] - k2 * acc.s[c / 3][c % 3];
+            Cx<float> v = ds(p.s[c / 3][c % 3]) - k2 * acc.s[c / 3][c % 3];
             acc.s[c / 3][c % 3] = v;
             n2 += (double)norm2(v);
         }
@@ -114,7 +117,7 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<float> ddp = d.s[c / 3][c % 3] - k2 * acc.s[c / 3][c % 3];
+            Cx<float> ddp = ds(d.s[c / 3][c % 3]) - k2 * acc.s[c / 3][c % 3];
             Cx<float> rv = r.s[c / 3][c % 3] - alpha * ddp;
             r.s[c / 3][c % 3] = rv;
             n2 += (double)norm2(rv);
@@ -140,6 +143,8 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
                                         double *red) {
     const double k2 = pr.kappa * pr.kappa;
     const bool solve = pr.mode == ENG_MODE_SOLVE;
+    const double dg = pr.diag;
+    auto ds = [dg](Cx<double> v) -> Cx<double> { return {__dmul_rn(dg, v.re), __dmul_rn(dg, v.im)}; };
     if (PHASE == PH_R2 || PHASE == PH_R4) {
         SpinorF64{pr.t64, stride}.store(i, acc);
     } else if (PHASE == PH_R3) {
@@ -150,7 +155,7 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
         if (solve) {
 #pragma unroll
             for (int c = 0; c < 12; c++) {
-                const Cx<double> mx = ldc(x, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+                const Cx<double> mx = ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3];
                 const Cx<double> bv = ldc(b, stride, c, i);
                 const Cx<double> sv = bv - mx;
                 stc(sp, stride, c, i, sv);
@@ -159,7 +164,7 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < 12; c++) stc(sp, stride, c, i, ldc(x, stride, c, i) - k2 * acc.s[c / 3][c % 3]);
+            for (int c = 0; c < 12; c++) stc(sp, stride, c, i, ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3]);
         }
         red[0] = n2;
         red[1] = d2;
@@ -171,7 +176,7 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
         if (solve) {
 #pragma unroll
             for (int c = 0; c < 12; c++) {
-                const Cx<double> v = ldc(sv, stride, c, i) - k2 * acc.s[c / 3][c % 3];
+                const Cx<double> v = ds(ldc(sv, stride, c, i)) - k2 * acc.s[c / 3][c % 3];
                 n2 += norm2(v);
                 rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};
             }
@@ -179,7 +184,7 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
 #pragma unroll
             for (int c = 0; c < 12; c++) {
                 const Cx<double> bv = ldc(b, stride, c, i);
-                const Cx<double> v = bv - (ldc(sv, stride, c, i) - k2 * acc.s[c / 3][c % 3]);
+                const Cx<double> v = bv - (ds(ldc(sv, stride, c, i)) - k2 * acc.s[c / 3][c % 3]);
                 d2 += norm2(bv);
                 n2 += norm2(v);
                 rl.s[c / 3][c % 3] = {(float)v.re, (float)v.im};

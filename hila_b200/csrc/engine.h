@@ -62,6 +62,7 @@ struct EngProblem {
     int lat;
     int mode;
     double kappa;
+    double diag;  // 1 + m_h: the Hasenbusch operator M + m_h (Hasenbusch.h:16-52); 1 for M
     // low precision (EVEN: p, r, Dp; ODD: t); FP16 fields carry a norm plane
     void *p, *r, *Dp, *t;
     float *pn, *rn, *Dpn, *tn;

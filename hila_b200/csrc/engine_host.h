@@ -36,8 +36,9 @@ class Engine {
 
     // Start a solve in a free slot.  b, x: FP64 EVEN halves (stride of the
     // lattice); null means slot-owned buffers (filled with upload_b / read with x_ptr).
+    // diag = 1 + m_h solves with the Hasenbusch operator M + m_h (1: M itself).
     int admit(int lat, double kappa, double2 *b, double2 *x, double tol, int maxiter, double delta, int mode,
-              int *slot);
+              int *slot, double diag = 1.0);
     double2 *own_b(int slot) { return bufs_[slot].b_own.as<double2>(); }
     double2 *own_x(int slot) { return bufs_[slot].x_own.as<double2>(); }
     int ensure_own(int slot);

@@ -43,50 +43,6 @@
 constexpr int kMmaBlockUnits = 98;
 constexpr int kMmaABytes = 4 * kMmaBlockUnits * 16;
 
-__device__ __forceinline__ unsigned h2_swap(unsigned x) { return __byte_perm(x, 0, 0x1032); }
-
-// x * phase, phase code 0: 1, 1: i, 2: -1, 3: -i; (re, im) in the low / high half
-template <int PH>
-__device__ __forceinline__ unsigned h2_phase(unsigned x) {
-    if constexpr (PH == 0)
-        return x;
-    else if constexpr (PH == 1)
-        return h2_swap(x) ^ 0x00008000u;  // i (re, im) = (-im, re)
-    else if constexpr (PH == 2)
-        return x ^ 0x80008000u;
-    else
-        return h2_swap(x) ^ 0x80000000u;  // -i (re, im) = (im, -re)
-}
-
-__device__ __forceinline__ unsigned h2_add(unsigned a, unsigned b) {
-    unsigned r;
-    asm("add.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned h2_mul(unsigned a, unsigned b) {
-    unsigned r;
-    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-    return r;
-}
-
-// Projection P_{mu,s} (h0 = w0 + ph0 w_pa0, h1 = w1 + ph1 w_pa1) and the lower
-// spins of E_{mu,s} (spin 2 = ps0 h_q0, spin 3 = ps1 h_q1), wilson_vector.h:439-567.
-template <int MU, int S>
-struct ProjTable {
-    static constexpr int pa0 = (MU == 0 || MU == 1) ? 3 : 2;
-    static constexpr int pa1 = (MU == 0 || MU == 1) ? 2 : 3;
-    static constexpr int ph0 = MU == 0 ? (S > 0 ? 1 : 3) : MU == 1 ? (S > 0 ? 2 : 0) : MU == 2 ? (S > 0 ? 1 : 3)
-                                                                                                : (S > 0 ? 0 : 2);
-    static constexpr int ph1 = MU == 0 ? (S > 0 ? 1 : 3) : MU == 1 ? (S > 0 ? 0 : 2) : MU == 2 ? (S > 0 ? 3 : 1)
-                                                                                                : (S > 0 ? 0 : 2);
-    static constexpr int q0 = (MU == 0 || MU == 1) ? 1 : 0;
-    static constexpr int q1 = (MU == 0 || MU == 1) ? 0 : 1;
-    static constexpr int ps0 = MU == 0 ? (S > 0 ? 3 : 1) : MU == 1 ? (S > 0 ? 0 : 2) : MU == 2 ? (S > 0 ? 3 : 1)
-                                                                                                : (S > 0 ? 0 : 2);
-    static constexpr int ps1 = MU == 0 ? (S > 0 ? 3 : 1) : MU == 1 ? (S > 0 ? 2 : 0) : MU == 2 ? (S > 0 ? 1 : 3)
-                                                                                                : (S > 0 ? 0 : 2);
-};
-
 // Stage one neighbour spinor of this lane's (site, source) for direction
 // (MU, B): load the FP16 spinor, project, scale by f2, and store the four A
 // rows (upper, lower spin pairs) at byte offset B * 16 of this lane's rows.

@@ -99,11 +99,11 @@ struct CgWorkspace {
     cudaGraphExec_t init_exec = nullptr, loop_exec = nullptr;
     struct Key {
         const void *gauge = nullptr, *in = nullptr, *out = nullptr;
-        double kappa = 0, acc2 = 0;
+        double kappa = 0, acc2 = 0, diag = 1;
         int maxiter = 0, mode = 0;
         bool operator==(const Key &o) const {
             return gauge == o.gauge && in == o.in && out == o.out && kappa == o.kappa && acc2 == o.acc2 &&
-                   maxiter == o.maxiter && mode == o.mode;
+                   diag == o.diag && maxiter == o.maxiter && mode == o.mode;
         }
     } key;
     bool allocated = false;
@@ -145,5 +145,8 @@ int ensure_reduction_capacity(hw_context *ctx, long nblocks);
 int ensure_stage(hw_context *ctx, size_t bytes);
 // pick the fastest FP64 hop launch shape for this lattice once (HW_HOP_VARIANT overrides)
 int tune_hop(hw_lattice *lat, const hw_gauge *G);
+// (M_s + m_h) on EVEN half fields (d = 1 + m_h), stream-ordered through the lattice's
+// ODD workspace field; context lock held, workspace and hop shape ready
+void eo_apply_half(const hw_gauge *G, double kappa, HalfF64 in, HalfF64 out, int sign, double d);
 void destroy_engines(hw_context *ctx);
 }  // namespace hw

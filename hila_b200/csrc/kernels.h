@@ -52,17 +52,20 @@ struct GaugeF64 {
 // out = a * H_s in
 void launch_hop_scale(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 out, double a,
                       const CgState *st, cudaStream_t s);
-// out = x + b * H_s in; with red != null also |out|^2 -> st->pAp and alpha = rr/pAp
+// The x-type term of the epilogues below carries a factor d (1 + m_h for the
+// Hasenbusch operator M + m_h, Hasenbusch.h:16-52; 1 for M itself).
+// out = d x + b * H_s in; with red != null also |out|^2 -> st->pAp and alpha = rr/pAp
 void launch_hop_xpay(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 x, HalfF64 out,
-                     double b, CgState *st, const RedBuf *red, cudaStream_t s);
+                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d = 1.0);
 // CG update fused into the last hop of M^dagger M p:
-//   DDp = Dp + b * H_s t;  r -= alpha DDp;  x += alpha p;  |r|^2 -> st (beta, status)
+//   DDp = d Dp + b * H_s t;  r -= alpha DDp;  x += alpha p;  |r|^2 -> st (beta, status)
 void launch_hop_cg_update(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 Dp,
                           HalfF64 r, HalfF64 x, HalfF64 p, double b, CgState *st, const RedBuf &red,
-                          cudaStream_t s);
-// explicit residual: res = src - (x + b * H_s t); |res|^2 -> st->res_num2, |src|^2 -> st->res_den2
+                          cudaStream_t s, double d = 1.0);
+// explicit residual: res = src - (d x + b * H_s t); |res|^2 -> st->res_num2, |src|^2 -> st->res_den2
 void launch_hop_residual(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 x,
-                         HalfF64 src, HalfF64 res, double b, CgState *st, const RedBuf &red, cudaStream_t s);
+                         HalfF64 src, HalfF64 res, double b, CgState *st, const RedBuf &red, cudaStream_t s,
+                         double d = 1.0);
 
 // ---- FP64 vector kernels over one half lattice
 // CG start: r = src - Ax (Ax may be null: x = 0), p = r; sets rr, src_norm2, target_rr, status

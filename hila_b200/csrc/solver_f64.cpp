@@ -34,6 +34,7 @@ struct F64Solve {
     const hw_gauge *G;
     CgWorkspace *w;
     double kappa;
+    double diag = 1.0;  // 1 + m_h: the Hasenbusch operator M + m_h (Hasenbusch.h:16-52)
     HalfF64 in;  // EVEN source of the normal system (MODE_NORMAL)
     HalfF64 b;   // EVEN right-hand side of M x = b (MODE_SOLVE)
     HalfF64 x;   // EVEN solution / initial guess
@@ -47,7 +48,7 @@ struct F64Solve {
     // out = M_sign v  (EVEN -> EVEN) through t (ODD)
     void M(int sign, HalfF64 v, HalfF64 out, CgState *pst, const RedBuf *r) {
         launch_hop_scale(lat->g, G->U(), 1, sign, v, w->t.h(), 1.0, nullptr, s);
-        launch_hop_xpay(lat->g, G->U(), 0, sign, w->t.h(), v, out, -kappa * kappa, pst, r, s);
+        launch_hop_xpay(lat->g, G->U(), 0, sign, w->t.h(), v, out, -kappa * kappa, pst, r, s, diag);
     }
 
     void enqueue_init(double acc2, int maxiter) {
@@ -60,10 +61,10 @@ struct F64Solve {
 
     void enqueue_body(cudaGraphConditionalHandle cond, int use_cond) {
         launch_hop_scale(lat->g, G->U(), 1, +1, w->p.h(), w->t.h(), 1.0, st, s);
-        launch_hop_xpay(lat->g, G->U(), 0, +1, w->t.h(), w->p.h(), w->Dp.h(), -kappa * kappa, st, &red, s);
+        launch_hop_xpay(lat->g, G->U(), 0, +1, w->t.h(), w->p.h(), w->Dp.h(), -kappa * kappa, st, &red, s, diag);
         launch_hop_scale(lat->g, G->U(), 1, -1, w->Dp.h(), w->t.h(), 1.0, st, s);
         launch_hop_cg_update(lat->g, G->U(), 0, -1, w->t.h(), w->Dp.h(), w->r.h(), x, w->p.h(), -kappa * kappa, st,
-                             red, s);
+                             red, s, diag);
         launch_cg_pupdate(lat->g.Vh, w->r.h(), w->p.h(), st, s);
         launch_loop_control(st, cond, use_cond, s);
     }
@@ -74,13 +75,13 @@ struct F64Solve {
             // |b - M x|
             launch_hop_scale(lat->g, G->U(), 1, +1, x, w->t.h(), 1.0, nullptr, s);
             launch_hop_residual(lat->g, G->U(), 0, +1, w->t.h(), x, b, HalfF64{nullptr, 0}, -kappa * kappa, st, red,
-                                s);
+                                s, diag);
         } else {
             // |in - M^dagger M x|
             M(+1, x, w->DDp.h(), nullptr, nullptr);
             launch_hop_scale(lat->g, G->U(), 1, -1, w->DDp.h(), w->t.h(), 1.0, nullptr, s);
             launch_hop_residual(lat->g, G->U(), 0, -1, w->t.h(), w->DDp.h(), in, HalfF64{nullptr, 0},
-                                -kappa * kappa, st, red, s);
+                                -kappa * kappa, st, red, s, diag);
         }
     }
 };
@@ -143,6 +144,7 @@ int run_f64(F64Solve &S, const hw_cg_params &P, hw_cg_result *R) {
     key.in = S.mode == MODE_SOLVE ? (const void *)S.b.p : (const void *)S.in.p;
     key.out = S.x.p;
     key.kappa = S.kappa;
+    key.diag = S.diag;
     key.acc2 = acc2;
     key.maxiter = P.maxiters;
     key.mode = S.mode;
@@ -242,6 +244,7 @@ int check_params(const hw_cg_params *p, hw_cg_params *out) {
     HW_CHECK_ARG(out->accuracy > 0 && std::isfinite(out->accuracy), "accuracy must be positive");
     HW_CHECK_ARG(out->maxiters > 0, "maxiters must be positive");
     HW_CHECK_ARG(out->precision >= HW_PREC_F64 && out->precision <= HW_PREC_F16, "unknown precision");
+    HW_CHECK_ARG(std::isfinite(out->hasenbusch_mh) && out->hasenbusch_mh > -1.0, "hasenbusch_mh must exceed -1");
     if (out->delta <= 0) out->delta = 0.1;
     return HW_OK;
 }
@@ -287,6 +290,7 @@ static int solve_common(const hw_gauge *G, double kappa, const hw_field *in, hw_
     S.G = G;
     S.w = lat->ws.get();
     S.kappa = kappa;
+    S.diag = 1.0 + P.hasenbusch_mh;
     S.in = in->half[0].h();
     S.b = in->half[0].h();
     S.x = out->half[0].h();

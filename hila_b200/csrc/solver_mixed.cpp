@@ -50,7 +50,7 @@ int mixed_solve(const hw_gauge *G, double kappa, const hw_field *src, hw_field *
     int slot;
     const int emode = mode == 1 ? ENG_MODE_SOLVE : ENG_MODE_NORMAL;
     if ((rc = E->admit(l, kappa, src->half[0].buf.as<double2>(), x->half[0].buf.as<double2>(), P.accuracy,
-                       P.maxiters, P.delta, emode, &slot)) != HW_OK)
+                       P.maxiters, P.delta, emode, &slot, 1.0 + P.hasenbusch_mh)) != HW_OK)
         return rc;
     HW_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     int chunks = 0;
@@ -102,6 +102,7 @@ int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_
         HW_CHECK_ARG(q.b->lat == q.gauge->lat && q.x->lat == q.gauge->lat, "request %d: lattice mismatch", k);
         HW_CHECK_ARG(q.b != q.x, "request %d: b and x must differ", k);
         HW_CHECK_ARG(q.accuracy > 0 && q.maxiters > 0, "request %d: bad accuracy or maxiters", k);
+        HW_CHECK_ARG(std::isfinite(q.hasenbusch_mh) && q.hasenbusch_mh > -1.0, "request %d: bad hasenbusch_mh", k);
     }
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     HW_CUDA(cudaSetDevice(ctx->device));
@@ -131,7 +132,7 @@ int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_
             if (E->free_slots_on(l) <= 0) break;
             int slot;
             if ((rc = E->admit(l, q.kappa, q.b->half[0].buf.as<double2>(), q.x->half[0].buf.as<double2>(),
-                               q.accuracy, q.maxiters, delta, ENG_MODE_SOLVE, &slot)) != HW_OK)
+                               q.accuracy, q.maxiters, delta, ENG_MODE_SOLVE, &slot, 1.0 + q.hasenbusch_mh)) != HW_OK)
                 return fail(rc);
             slot_of[next] = slot;
             next++;

@@ -131,6 +131,22 @@ int hw_wilson_evenodd_apply(const hw_gauge *gauge, double kappa, const hw_field 
 /* Dirac_Wilson_evenodd::dagger(in, out), wilson.h:282-289 (sign -1) */
 int hw_wilson_evenodd_dagger(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out);
 
+/* Hasenbusch_operator<Dirac_Wilson_evenodd>::apply / dagger, Hasenbusch.h:39-47:
+ * out = (M_s + m_h) in on EVEN (sign +1 apply, -1 dagger), out[ODD] = 0.  Its
+ * force is the operator's (Hasenbusch.h:49-52, hw_wilson_evenodd_force); its
+ * inverse comes from the solvers with hw_cg_params.hasenbusch_mh / hw_solve_request.hasenbusch_mh. */
+int hw_hasenbusch_evenodd_apply(const hw_gauge *gauge, double kappa, double mh, const hw_field *in, hw_field *out);
+int hw_hasenbusch_evenodd_dagger(const hw_gauge *gauge, double kappa, double mh, const hw_field *in, hw_field *out);
+
+/* MRE_guess(psi, chi, D, old_chi_inv), MRE_guess.h:9-88: initial guess psi for
+ * the normal system (M + m_h)^dag (M + m_h) psi = chi from n earlier solutions
+ * old[0..n-1]: the minimal-residual combination over their orthogonalised span
+ * (real coefficients from Re<.,.> over EVEN, as the reference; the reference's
+ * Gram-Schmidt and final accumulation are written as intended, not as its
+ * text, which overwrites psi in its last loop).  m_h = 0 for M itself. */
+int hw_mre_guess(const hw_gauge *gauge, double kappa, double mh, const hw_field *const *old, int n,
+                 const hw_field *chi, hw_field *psi);
+
 /* Dirac_Wilson_evenodd::force(chi, psi, force, sign), wilson.h:293-311 (with
  * Dirac_Wilson_calc_force, wilson.h:110-137): the derivative of
  * Re(chi^dag M_s psi) (chi, psi on EVEN) with respect to every link, as 3x3
@@ -182,6 +198,7 @@ typedef struct hw_cg_params {
     int true_residual;   /* 1: stop only when the explicitly recomputed FP64 residual meets
                             accuracy; 0: reference stopping rule on the iterated residual */
     int use_graph;       /* 1: device-resident iteration in a CUDA graph (default); 0: host loop */
+    double hasenbusch_mh; /* m_h of the Hasenbusch operator M + m_h (Hasenbusch.h:16-52); 0: M itself */
 } hw_cg_params;
 
 typedef struct hw_cg_result {
@@ -228,6 +245,7 @@ typedef struct hw_solve_request {
     hw_field *x;           /* solution; holds the initial guess on entry */
     double accuracy;       /* stop when |b - M x| / |b| <= accuracy (FP64, recomputed) */
     int maxiters;
+    double hasenbusch_mh;  /* solve (M + m_h) x = b instead (Hasenbusch.h:16-52); 0: M */
 } hw_solve_request;
 
 /* Many right-hand sides on many lattices at once (no reference counterpart:

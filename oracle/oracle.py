@@ -160,6 +160,69 @@ def eo_force(dims, U, kappa, chi, psi, sign=1, antiperiodic=True) -> np.ndarray:
     return out
 
 
+def hasenbusch_eo_apply(dims, U, kappa, mh, inp, sign=1, antiperiodic=True):
+    """Hasenbusch_operator::apply / dagger (Hasenbusch.h:39-47): (M_s + m_h) inp on EVEN."""
+    out = eo_apply(dims, U, kappa, inp, sign, antiperiodic)
+    even = parity_mask(dims) == 0
+    out[even] += mh * inp[even]
+    return out
+
+
+def parity_mask(dims) -> np.ndarray:
+    """(x + y + z + t) mod 2 per lexicographic site."""
+    x, y, z, t = np.meshgrid(*[np.arange(d) for d in dims], indexing="ij")
+    return ((x + y + z + t) % 2).transpose(3, 2, 1, 0).reshape(-1)
+
+
+def mre_guess(dims, U, kappa, mh, old, chi, antiperiodic=True) -> np.ndarray:
+    """MRE_guess (MRE_guess.h:9-88) with the intended Gram-Schmidt (overlap over |b_j|^2)
+    and accumulation psi = sum_i v_i b_i; real inner products over EVEN (rdot)."""
+    even = parity_mask(dims) == 0
+
+    def rdot(a, b):
+        return float(np.sum(a[even] * b[even]))
+
+    def A(v):
+        w = hasenbusch_eo_apply(dims, U, kappa, mh, v, +1, antiperiodic)
+        return hasenbusch_eo_apply(dims, U, kappa, mh, w, -1, antiperiodic)
+
+    n = len(old)
+    basis = []
+    for i in range(n):
+        b = np.array(old[i], np.float64, copy=True)
+        b[~even] = 0.0
+        for bj in basis:
+            nj = rdot(bj, bj)
+            if nj > 1e-300:
+                b -= rdot(bj, b) / nj * bj
+        basis.append(b)
+    M = np.zeros((n, n))
+    v = np.zeros(n)
+    for i in range(n):
+        Ab = A(basis[i])
+        for j in range(n):
+            M[j, i] = rdot(basis[j], Ab)
+        v[i] = rdot(basis[i], chi)
+    for i in range(n):  # Gauss-Jordan as MRE_guess.h:55-80
+        if M[i, i] * M[i, i] > 1e-32:
+            inv = 1.0 / M[i, i]
+            M[i, :] *= inv
+            v[i] *= inv
+            for k in range(n):
+                if k != i:
+                    w = M[k, i]
+                    M[k, :] -= w * M[i, :]
+                    v[k] -= w * v[i]
+        else:
+            v[i] = 0.0
+            M[:, i] = 0.0
+    psi = np.zeros_like(np.asarray(chi, np.float64))
+    for i in range(n):
+        if np.isfinite(v[i]) and v[i] != 0.0:
+            psi += v[i] * basis[i]
+    return psi
+
+
 def true_residual(dims, U, kappa, b, x, sign=1, antiperiodic=True) -> float:
     return lib().or_true_residual(_dims(dims), int(antiperiodic), _d(U), kappa, _d(b), _d(x), sign)
 
