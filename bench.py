@@ -199,8 +199,9 @@ def engine_phase_bytes(phase: str, vh: int, nrhs: int, prec: str, link_format: i
     lk = 8 * (36 if prec == "f16" else 48)
     lk64 = 8 * (144 if link_format == 18 else 96)
     per = {"P1": (2 * sp, lk), "P2": (3 * sp, lk), "P3": (2 * sp, lk), "P4": (6 * sp + 2 * 96, lk),
-           "R1": (2 * 192 + 2 * 96, 0), "R2": (2 * 192, lk64), "R3": (4 * 192, lk64),
-           "R4": (2 * 192, lk64), "R5": (2 * 192 + sp, lk64), "P5": (3 * sp, 0)}
+           "R1": (2 * 192 + 2 * 96, 0), "R2": (2 * 192, lk64), "R3": (4 * 192 + sp, lk64),
+           "R4": (2 * 192, lk64), "R4L": (2 * sp, lk), "R5": (3 * 192 + sp, lk64), "R5L": (3 * sp, lk),
+           "P5": (3 * sp, 0)}
     pair, links = per[phase]
     return int(vh * (nrhs * pair + links))
 

@@ -85,7 +85,7 @@ class _RequestResult(ctypes.Structure):
 
 
 class _EngineProfile(ctypes.Structure):
-    _fields_ = [("launches", ctypes.c_int * 10), ("ms", ctypes.c_double * 10)]
+    _fields_ = [("launches", ctypes.c_int * 12), ("ms", ctypes.c_double * 12)]
 
 
 class _ServerStats(ctypes.Structure):
@@ -284,7 +284,7 @@ class Context:
     def synchronize(self):
         _check(lib().hw_context_synchronize(self.handle))
 
-    ENGINE_PHASES = ("P1", "P2", "P3", "P4", "R1", "R2", "R3", "R4", "R5", "P5")
+    ENGINE_PHASES = ("P1", "P2", "P3", "P4", "R1", "R2", "R3", "R4", "R4L", "R5", "R5L", "P5")
 
     def engine_profile(self, enable: bool) -> None:
         """Per-phase event timing of the batched engines (hw_engine_profile_enable)."""

@@ -281,6 +281,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     EngState &S = host_states_[slot];
     std::memset(&S, 0, sizeof(S));
     S.status = ENG_RUNNING;
+    S.mode = mode;
     S.ru = 1;
     S.init = 1;
     S.tol2 = tol * tol;
@@ -433,7 +434,7 @@ int Engine::launch_chunk_profiled(int iters) {
         for (int j = 0; j < kEngMaxProb; j++)
             if (slots_[j].used) ru_after += host_states_[j].n_ru;
         for (int ph = 0; ph < kEngPhases; ph++) {
-            const bool ru_phase = ph >= PH_R1 && ph <= PH_R5;
+            const bool ru_phase = eng_ru_phase(ph);
             if (ru_phase && ru_after == ru_before) continue;
             if (ph <= PH_P4 && inner == 0) continue;
             float ms = 0.f;

@@ -71,7 +71,9 @@ __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
 // which run after every tile of the lattice is done, so all blocks agree.
 template <int PHASE>
 __device__ __forceinline__ bool active(const EngState &s) {
-    if (PHASE >= PH_R1 && PHASE <= PH_R5) return s.ru != 0;
+    if (PHASE == PH_R4 || PHASE == PH_R5) return s.ru != 0 && s.mode == ENG_MODE_NORMAL;
+    if (PHASE == PH_R4L || PHASE == PH_R5L) return s.ru != 0 && s.mode == ENG_MODE_SOLVE;
+    if (eng_ru_phase(PHASE)) return s.ru != 0;
     return s.status == ENG_RUNNING && s.ru == 0;
 }
 
@@ -93,8 +95,22 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
     // d p as an uncontracted product: with d = 1 the sums round exactly as p - k^2 acc
     const float dg = (float)pr.diag;
     auto ds = [dg](Cx<float> v) -> Cx<float> { return {__fmul_rn(dg, v.re), __fmul_rn(dg, v.im)}; };
-    if (PHASE == PH_P1 || PHASE == PH_P3) {
+    if (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R4L) {
         L::sp(pr.t, pr.tn, stride).store(i, acc);
+    } else if (PHASE == PH_R5L) {
+        // r = d s - k^2 H^dag t with s_low in Dp (reliable update of M x = b); |r|^2
+        const float k2 = (float)(pr.kappa * pr.kappa);
+        Spinor<float> sv;
+        L::sp(pr.Dp, pr.Dpn, stride).load_cached(i, sv);
+        double n2 = 0;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            Cx<float> v = ds(sv.s[c / 3][c % 3]) - k2 * acc.s[c / 3][c % 3];
+            acc.s[c / 3][c % 3] = v;
+            n2 += (double)norm2(v);
+        }
+        L::sp(pr.r, pr.rn, stride).store(i, acc);
+        red[0] = n2;
     } else if (PHASE == PH_P2) {
         const float k2 = (float)(pr.kappa * pr.kappa);
         Spinor<float> p;
@@ -153,15 +169,18 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
         double2 *__restrict__ sp = pr.s;
         double n2 = 0, d2 = 0;
         if (solve) {
+            Spinor<float> sl;
 #pragma unroll
             for (int c = 0; c < 12; c++) {
                 const Cx<double> mx = ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3];
                 const Cx<double> bv = ldc(b, stride, c, i);
                 const Cx<double> sv = bv - mx;
                 stc(sp, stride, c, i, sv);
+                sl.s[c / 3][c % 3] = {(float)sv.re, (float)sv.im};
                 n2 += norm2(sv);
                 d2 += norm2(bv);
             }
+            Low<LOW>::sp(pr.Dp, pr.Dpn, stride).store(i, sl);  // input of R4L / R5L
         } else {
 #pragma unroll
             for (int c = 0; c < 12; c++) stc(sp, stride, c, i, ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3]);
@@ -231,9 +250,9 @@ __device__ void finish(EngState &s, const EngProblem &pr, const double *tot, int
             s.s2 = tot[0];
             s.b2 = tot[1];
         }
-    } else if (PHASE == PH_R5) {
+    } else if (PHASE == PH_R5 || PHASE == PH_R5L) {
         const double r2 = tot[0];
-        if (pr.mode == ENG_MODE_NORMAL) {
+        if (PHASE == PH_R5 && pr.mode == ENG_MODE_NORMAL) {
             s.b2 = tot[1];
             s.s2 = r2;
         }
@@ -309,9 +328,10 @@ __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLat
 template <int PHASE, int LOW, int NR, int MINB, bool FULL18>
 __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
     constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2) ? 1 : -1;
-    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3) ? 1 : 0;
-    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4) ? 1 : 0;
+    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R4L) ? 1 : 0;
+    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4 || PHASE == PH_R5L) ? 1 : 0;
     using L = Low<LOW>;
+    if (eng_ru_phase(PHASE) && *(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
     __shared__ double smem[kEngTile / 32];
     __shared__ bool last;
     __shared__ int s_act[kEngMaxRhs];
@@ -345,8 +365,9 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 const EngProblem &pr = T->prob[s_act[g0 + min(r, cnt - 1)]];
-                void *ip = (PHASE == PH_P1) ? pr.p : (PHASE == PH_P3 ? pr.Dp : pr.t);
-                float *inn = (PHASE == PH_P1) ? pr.pn : (PHASE == PH_P3 ? pr.Dpn : pr.tn);
+                constexpr bool from_dp = PHASE == PH_P3 || PHASE == PH_R4L;
+                void *ip = (PHASE == PH_P1) ? pr.p : (from_dp ? pr.Dp : pr.t);
+                float *inn = (PHASE == PH_P1) ? pr.pn : (from_dp ? pr.Dpn : pr.tn);
                 in[r] = L::sp(ip, inn, stride);
             }
             Spinor<float> acc[NR];
@@ -604,22 +625,35 @@ inline void mark(const cudaEvent_t *ev, int k, cudaStream_t s) {
     if (ev) cudaEventRecord(ev[k], s);
 }
 
-// R1..R5 and P5 (phases 4..9), shared by every launch shape of the inner phases
-template <int LOW>
+// R1..R5L and P5 (phases 4..11), shared by every launch shape of the inner phases;
+// LowRU launches R4L / R5L in the inner phases' shape
+template <int LOW, class LowRU>
 void enqueue_reliable_update(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     k_eng_vec<PH_R1, LOW><<<G.low, kEngTile, 0, s>>>(P);
-    mark(ev, 5, s);
+    mark(ev, PH_R2, s);
     launch_f64<PH_R2, LOW>(P, G, s);
-    mark(ev, 6, s);
+    mark(ev, PH_R3, s);
     launch_f64<PH_R3, LOW>(P, G, s);
-    mark(ev, 7, s);
+    mark(ev, PH_R4, s);
     launch_f64<PH_R4, LOW>(P, G, s);
-    mark(ev, 8, s);
+    mark(ev, PH_R4L, s);
+    LowRU::template launch<PH_R4L>(P, G, s);
+    mark(ev, PH_R5, s);
     launch_f64<PH_R5, LOW>(P, G, s);
-    mark(ev, 9, s);
+    mark(ev, PH_R5L, s);
+    LowRU::template launch<PH_R5L>(P, G, s);
+    mark(ev, PH_P5, s);
     k_eng_vec<PH_P5, LOW><<<G.low, kEngTile, 0, s>>>(P);
-    mark(ev, 10, s);
+    mark(ev, kEngPhases, s);
 }
+
+template <int LOW, int NR, int MINB, bool FULL18>
+struct LowShape {
+    template <int PHASE>
+    static void launch(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+        k_eng_low<PHASE, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    }
+};
 
 template <int LOW, int NR, int MINB, bool FULL18>
 void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
@@ -632,7 +666,7 @@ void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s, con
     mark(ev, 3, s);
     k_eng_low<PH_P4, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 4, s);
-    enqueue_reliable_update<LOW>(P, G, s, ev);
+    enqueue_reliable_update<LOW, LowShape<LOW, NR, MINB, FULL18>>(P, G, s, ev);
 }
 
 constexpr int kMmaMinBlocks = 4;
@@ -648,7 +682,7 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
     mark(ev, 3, s);
     k_eng_mma<PH_P4, kMmaMinBlocks><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 4, s);
-    enqueue_reliable_update<LOW_F16>(P, G, s, ev);
+    enqueue_reliable_update<LOW_F16, LowShape<LOW_F16, 1, 6, true>>(P, G, s, ev);
 }
 
 // Launch shapes of the low-precision phases (EngGrid::variant):

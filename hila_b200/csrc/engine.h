@@ -18,11 +18,12 @@
 // Reliable update (FP64, only slots that asked for it):
 //   R1  x += y; y = 0                          (FP64 solution accumulation)
 //   R2  t64 = H^{oe}_+ x
-//   R3  solve mode:  s = b - (x - kappa^2 H t64)   |s|^2, |b|^2
+//   R3  solve mode:  s = b - (x - kappa^2 H t64)   |s|^2, |b|^2; s also in low precision (Dp)
 //       normal mode: s = x - kappa^2 H t64         (= M x)
-//   R4  t64 = H^{oe}_- s
-//   R5  solve mode:  r = s - kappa^2 H^dag t64      (= M^dag (b - M x))
-//       normal mode: r = b - (s - kappa^2 H^dag t64) (= b - M^dag M x), |b|^2
+//   R4  normal mode: t64 = H^{oe}_- s
+//   R4L solve mode:  t = H^{oe}_- s_low            (low precision)
+//   R5  normal mode: r = b - (s - kappa^2 H^dag t64) (= b - M^dag M x), |b|^2
+//   R5L solve mode:  r = s_low - kappa^2 H^dag t    (= M^dag (b - M x), low precision)
 //       r_low = r, |r|^2 -> true residual, convergence, beta
 //   P5  p = r + beta p   (p = r on a slot's first iteration)
 #pragma once
@@ -88,7 +89,8 @@ struct EngState {
     int ru;          // 1: reliable update pending
     int init;        // 1: first reliable update (r from x), p = r afterwards
     int n_ru;
-    int pad[2];
+    int mode;        // EngMode of the slot (copy of its problem's, read by the phase selection)
+    int pad;
 };
 
 struct EngTables {
@@ -119,8 +121,14 @@ struct EngGrid {
     int planes_mask;  // FP64 link formats present: bit 0 = 18 reals, bit 1 = 12 reals
 };
 
-enum EngPhase : int { PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R5, PH_P5 };
-constexpr int kEngPhases = 10;
+// in launch order; R4 / R5 serve slots of the normal system (FP64), R4L / R5L those of
+// M x = b (low precision: r = M^dag s only feeds the low-precision iteration, and s
+// = b - M x, on which convergence is decided, stays FP64)
+enum EngPhase : int {
+    PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R4L, PH_R5, PH_R5L, PH_P5
+};
+constexpr int kEngPhases = 12;
+constexpr bool eng_ru_phase(int ph) { return ph >= PH_R1 && ph <= PH_R5L; }
 
 // low-precision format of one engine (template parameter of the inner phases)
 enum EngLow : int { LOW_F32 = 1, LOW_F16 = 2 };

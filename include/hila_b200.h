@@ -325,10 +325,12 @@ int hw_server_stats_get(hw_server *server, hw_server_stats *stats);
  * CUDA events around every phase launch (the reference has no counterpart; it
  * times whole calls, bench_fermion.cpp:95-120).  While enabled, iterations run
  * from a host loop that synchronises after each one, so solves are slower; the
- * phase times are those of the same kernels.  Phases 0..9: P1 t = H p, P2
+ * phase times are those of the same kernels.  Phases 0..11: P1 t = H p, P2
  * Dp = M p and |Dp|^2, P3 t = H^dag Dp, P4 r -= alpha M^dag Dp, y += alpha p,
- * |r|^2, R1..R5 the FP64 reliable update, P5 p = r + beta p. */
-#define HW_ENGINE_PHASES 10
+ * |r|^2; the reliable update R1 x += y, R2 and R3 s = b - M x in FP64, then
+ * r = M^dag s by R4, R5 (FP64, normal system) or R4L, R5L (low precision,
+ * M x = b); P5 p = r + beta p. */
+#define HW_ENGINE_PHASES 12
 typedef struct hw_engine_profile {
     int launches[HW_ENGINE_PHASES]; /* launches that had work */
     double ms[HW_ENGINE_PHASES];    /* their summed device time */
