@@ -452,10 +452,10 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
             Spinor<double> acc;
 #pragma unroll
             for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {0.0, 0.0};
-            hop_dir<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir_lean<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir_lean<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir_lean<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            hop_dir_lean<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
             epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
         }
         if constexpr (NRED > 0) {

@@ -128,7 +128,7 @@ enum EngPhase : int {
     PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R4L, PH_R5, PH_R5L, PH_P5
 };
 constexpr int kEngPhases = 12;
-constexpr bool eng_ru_phase(int ph) { return ph >= PH_R1 && ph <= PH_R5L; }
+__host__ __device__ constexpr bool eng_ru_phase(int ph) { return ph >= PH_R1 && ph <= PH_R5L; }
 
 // low-precision format of one engine (template parameter of the inner phases)
 enum EngLow : int { LOW_F32 = 1, LOW_F16 = 2 };

@@ -414,6 +414,47 @@ __device__ __forceinline__ void hop_dir_multi(const SiteNbrs &n, int par, int i,
     }
 }
 
+// hop_dir with one colour-multiplied half spinor live at a time (expand_add_half):
+// the same arithmetic in the same order, fewer registers
+template <int MU, int SIGN, class SpIn, class Lk, typename R>
+__device__ __forceinline__ void hop_dir_lean(const SiteNbrs &n, int par, int i, const SpIn &in, const Lk &U,
+                                             Spinor<R> &acc) {
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+        Cx<R> h0[3], h1[3], v[3];
+        {
+            Spinor<R> w;
+            in.load(b == 0 ? n.fwd[MU] : n.bwd[MU], w);
+            if (b == 0)
+                project<MU, SIGN>(w, h0, h1);
+            else
+                project<MU, -SIGN>(w, h0, h1);
+            if (MU == 3) {
+                const R sg = (b == 0 ? n.tfwd_wrap : n.tbwd_wrap) ? R(-1) : R(1);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    h0[k] = sg * h0[k];
+                    h1[k] = sg * h1[k];
+                }
+            }
+        }
+        Su3<R> u;
+        if (b == 0) {
+            U.load(par, MU, i, u);
+            su3_mul(u, h0, v);
+            expand_add_half<MU, SIGN, 0>(acc, v);
+            su3_mul(u, h1, v);
+            expand_add_half<MU, SIGN, 1>(acc, v);
+        } else {
+            U.load(1 - par, MU, n.bwd[MU], u);
+            su3_adj_mul(u, h0, v);
+            expand_add_half<MU, -SIGN, 0>(acc, v);
+            su3_adj_mul(u, h1, v);
+            expand_add_half<MU, -SIGN, 1>(acc, v);
+        }
+    }
+}
+
 template <int SIGN, class SpIn, class Lk, typename R>
 __device__ __forceinline__ void hop_site(const Geom &g, int par, int i, const SpIn &in, const Lk &U,
                                          Spinor<R> &acc) {

@@ -213,6 +213,36 @@ __device__ __forceinline__ void expand_add(Spinor<R> &acc, const Cx<R> h0[3], co
     }
 }
 
+// The contributions of one projected component to E_{dir,sign}: Q = 0 adds h0
+// (spin 0 and the lower spin built from h0), Q = 1 adds h1.  expand_add<DIR,
+// SIGN>(acc, h0, h1) equals expand_add_half<DIR, SIGN, 0>(acc, h0) followed by
+// expand_add_half<DIR, SIGN, 1>(acc, h1), element by element (each element of
+// acc receives one term), so a hop can hold one of h0, h1 at a time.
+template <int DIR, int SIGN, int Q, typename R>
+__device__ __forceinline__ void expand_add_half(Spinor<R> &acc, const Cx<R> h[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        acc.s[Q][k] = acc.s[Q][k] + h[k];
+        if (DIR == 0) {  // r2 = -s i h1, r3 = -s i h0
+            Cx<R> &lo = acc.s[Q == 0 ? 3 : 2][k];
+            lo = SIGN > 0 ? lo - mul_i(h[k]) : lo + mul_i(h[k]);
+        } else if (DIR == 1) {  // r2 = s h1, r3 = -s h0
+            if (Q == 0)
+                acc.s[3][k] = SIGN > 0 ? acc.s[3][k] - h[k] : acc.s[3][k] + h[k];
+            else
+                acc.s[2][k] = SIGN > 0 ? acc.s[2][k] + h[k] : acc.s[2][k] - h[k];
+        } else if (DIR == 2) {  // r2 = -s i h0, r3 = s i h1
+            if (Q == 0)
+                acc.s[2][k] = SIGN > 0 ? acc.s[2][k] - mul_i(h[k]) : acc.s[2][k] + mul_i(h[k]);
+            else
+                acc.s[3][k] = SIGN > 0 ? acc.s[3][k] + mul_i(h[k]) : acc.s[3][k] - mul_i(h[k]);
+        } else {  // r2 = s h0, r3 = s h1
+            Cx<R> &lo = acc.s[Q == 0 ? 2 : 3][k];
+            lo = SIGN > 0 ? lo + h[k] : lo - h[k];
+        }
+    }
+}
+
 // a + s v and a + s (i v), component-wise FMAs
 template <typename R>
 __device__ __forceinline__ Cx<R> axpy(Cx<R> a, R s, Cx<R> v) {
