@@ -136,6 +136,14 @@ _SIGNATURES = {
     "hw_hasenbusch_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp]),
     "hw_mre_guess": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(_vp), ctypes.c_int, _vp,
                                     _vp]),
+    "hw_stag_field_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "hw_stag_field_destroy": (ctypes.c_int, [_vp]),
+    "hw_stag_field_upload": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_stag_field_download": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_staggered_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "hw_staggered_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "hw_staggered_evenodd_force": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, _dp]),
+    "hw_staggered_cg_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, _vp, _vp]),
     "hw_gauge_config_dims": (ctypes.c_int, [ctypes.c_char_p, _ip]),
     "hw_gauge_config_write": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
     "hw_gauge_config_read": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
@@ -459,6 +467,73 @@ class Dirac_Wilson_evenodd:
         r = _CgResult()
         rc = lib().hw_wilson_evenodd_solve_host(self.gauge.handle, self.kappa, _dptr(b), _dptr(x), ctypes.byref(p),
                                                 ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        return CGResult.from_c(r)
+
+
+class StaggeredField:
+    """Field<SU_vector<3,double>> for staggered fermions; host arrays (V, 3, 2)."""
+
+    def __init__(self, lattice: Lattice, data: np.ndarray | None = None, parity: int = ALL):
+        self.lattice = lattice
+        self.handle = _vp()
+        _check(lib().hw_stag_field_create(lattice.handle, ctypes.byref(self.handle)))
+        lattice._adopt(self)
+        if data is not None:
+            self.upload(data, parity)
+
+    def upload(self, data: np.ndarray, parity: int = ALL):
+        data = np.ascontiguousarray(data, np.float64)
+        if data.size != self.lattice.volume * 6:
+            raise ValueError("staggered arrays hold V*6 doubles")
+        _check(lib().hw_stag_field_upload(self.handle, _dptr(data), int(parity)))
+
+    def download(self, parity: int = ALL) -> np.ndarray:
+        out = np.zeros((self.lattice.volume, 3, 2), np.float64)
+        _check(lib().hw_stag_field_download(self.handle, _dptr(out), int(parity)))
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().hw_stag_field_destroy(self.handle)
+            self.handle = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class dirac_staggered_evenodd:
+    """dirac_staggered_evenodd<SU<3,double>> (staggered.h:174-265) on EVEN."""
+
+    par = EVEN
+
+    def __init__(self, mass: float, gauge: GaugeField):
+        self.mass = float(mass)
+        self.gauge = gauge
+
+    def apply(self, inp: StaggeredField, out: StaggeredField):
+        _check(lib().hw_staggered_evenodd_apply(self.gauge.handle, self.mass, inp.handle, out.handle))
+
+    def dagger(self, inp: StaggeredField, out: StaggeredField):
+        _check(lib().hw_staggered_evenodd_dagger(self.gauge.handle, self.mass, inp.handle, out.handle))
+
+    def force(self, chi: StaggeredField, psi: StaggeredField, sign: int = 1) -> np.ndarray:
+        out = np.zeros((4, self.gauge.lattice.volume, 3, 3, 2), np.float64)
+        _check(lib().hw_staggered_evenodd_force(self.gauge.handle, self.mass, chi.handle, psi.handle, int(sign),
+                                                _dptr(out)))
+        return out
+
+    def cg(self, inp: StaggeredField, out: StaggeredField, accuracy: float = 1e-12, maxiters: int = 10000,
+           true_residual: bool = False) -> "CGResult":
+        """CG<dirac_staggered_evenodd>::apply: M^dag M out = inp, out the initial guess."""
+        p = _params(accuracy, maxiters, "f64", 0.1, true_residual, False)
+        r = _CgResult()
+        rc = lib().hw_staggered_cg_solve(self.gauge.handle, self.mass, inp.handle, out.handle, ctypes.byref(p),
+                                         ctypes.byref(r))
         if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
             _check(rc)
         return CGResult.from_c(r)

@@ -331,6 +331,17 @@ struct SiteNbrs {
     bool tfwd_wrap, tbwd_wrap;
 };
 
+// coordinates (x, y, z, t) of checkerboard site i of parity par
+__device__ __forceinline__ void site_coords(const Geom &g, int i, int par, int c[4]) {
+    const int q1 = (int)g.dx.div((unsigned)i);
+    const int xh = i - q1 * g.lxh;
+    const int q2 = (int)g.dy.div((unsigned)q1);
+    c[1] = q1 - q2 * g.L[1];
+    c[3] = (int)g.dz.div((unsigned)q2);
+    c[2] = q2 - c[3] * g.L[2];
+    c[0] = 2 * xh + ((c[1] + c[2] + c[3] + par) & 1);
+}
+
 // neighbours of checkerboard site i of parity par
 __device__ __forceinline__ SiteNbrs site_neighbours(const Geom &g, int i, int par) {
     SiteNbrs n;

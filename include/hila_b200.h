@@ -318,6 +318,33 @@ int hw_server_wait(hw_server *server, uint64_t request_id, double *const *soluti
 int hw_server_cancel(hw_server *server, uint64_t request_id);
 int hw_server_stats_get(hw_server *server, hw_server_stats *stats);
 
+/* ------------------------------------------------------------------ staggered fermions */
+
+/* Field<SU_vector<3,double>> for staggered fermions (libraries/dirac/staggered.h):
+ * host layout double[V][3][2] (colour-vector complex, lexicographic). */
+typedef struct hw_stag_field hw_stag_field;
+int hw_stag_field_create(hw_lattice *lat, hw_stag_field **field);  /* zero-filled */
+int hw_stag_field_destroy(hw_stag_field *field);
+int hw_stag_field_upload(hw_stag_field *field, const double *host, int parity);
+/* sites of the parities not requested come back as zero */
+int hw_stag_field_download(const hw_stag_field *field, double *host, int parity);
+
+/* dirac_staggered_evenodd<SU<3,double>>::apply / dagger, staggered.h:224-242:
+ * out[EVEN] = m in_e + D_eo (1/m) D_oe in_e with D = 0.5 s sum_mu eta_mu (U fwd -
+ * U^dag bwd) (staggered.h:48-68, eta as staggered.h:14-28 codes it); out[ODD]
+ * keeps (1/m) D_oe in_e as the reference leaves it.  Stream-ordered. */
+int hw_staggered_evenodd_apply(const hw_gauge *gauge, double mass, const hw_stag_field *in, hw_stag_field *out);
+int hw_staggered_evenodd_dagger(const hw_gauge *gauge, double mass, const hw_stag_field *in, hw_stag_field *out);
+/* dirac_staggered_evenodd::force(chi, psi, force, sign), staggered.h:246-265 and
+ * :70-86, in the host link layout double[4][V][3][3][2].  Synchronises. */
+int hw_staggered_evenodd_force(const hw_gauge *gauge, double mass, const hw_stag_field *chi, const hw_stag_field *psi,
+                               int sign, double *force);
+/* CG<dirac_staggered_evenodd>::apply, conjugate_gradient.h:46-104: M^dag M out = in
+ * on EVEN, out the initial guess; FP64 (params->precision must be HW_PREC_F64);
+ * result reports the recomputed |in - M^dag M out| / |in|. */
+int hw_staggered_cg_solve(const hw_gauge *gauge, double mass, const hw_stag_field *in, hw_stag_field *out,
+                          const hw_cg_params *params, hw_cg_result *result);
+
 /* ------------------------------------------------------------------ profiling */
 
 /* Device time per phase of the batched mixed-precision engines behind

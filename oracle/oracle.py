@@ -57,6 +57,9 @@ def lib():
             "or_wilson_apply": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int]),
             "or_wilson_eo_apply": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int]),
             "or_wilson_eo_force": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int, _dp]),
+            "or_staggered_hop": (v, [_ip, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]),
+            "or_staggered_eo_apply": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int]),
+            "or_staggered_eo_force": (v, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp, ctypes.c_int, _dp]),
             "or_dot": (v, [_ip, _dp, _dp, ctypes.c_int, _dp, _dp]),
             "or_squarenorm": (ctypes.c_double, [_ip, _dp, ctypes.c_int]),
             "or_cg": (ctypes.c_int, [_ip, ctypes.c_int, _dp, ctypes.c_double, _dp, _dp,
@@ -221,6 +224,33 @@ def mre_guess(dims, U, kappa, mh, old, chi, antiperiodic=True) -> np.ndarray:
         if np.isfinite(v[i]) and v[i] != 0.0:
             psi += v[i] * basis[i]
     return psi
+
+
+def staggered_eo_apply(dims, U, mass, inp, sign=1, antiperiodic=True) -> np.ndarray:
+    """dirac_staggered_evenodd::apply / dagger (staggered.h:224-242) on colour-vector fields
+    (V, 3, 2); out[ODD] keeps (1/m) D_oe in as the reference leaves it."""
+    inp = np.ascontiguousarray(inp, np.float64)
+    out = np.zeros_like(inp)
+    lib().or_staggered_eo_apply(_dims(dims), int(antiperiodic), _d(U), mass, _d(inp), _d(out), sign)
+    return out
+
+
+def staggered_eo_force(dims, U, mass, chi, psi, sign=1, antiperiodic=True) -> np.ndarray:
+    """dirac_staggered_evenodd::force (staggered.h:246-265), shape (4, V, 3, 3, 2)."""
+    chi = np.ascontiguousarray(chi, np.float64)
+    psi = np.ascontiguousarray(psi, np.float64)
+    out = np.zeros((4, volume(dims), 3, 3, 2))
+    lib().or_staggered_eo_force(_dims(dims), int(antiperiodic), _d(U), mass, _d(chi), _d(psi), sign, _d(out))
+    return out
+
+
+def gen_colour_vector(dims, seed: int, parity: int = ALL) -> np.ndarray:
+    """Gaussian colour-vector field (V, 3, 2), zero outside `parity` (tests only)."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((volume(dims), 3, 2))
+    if parity != ALL:
+        v[parity_mask(dims) != (0 if parity == EVEN else 1)] = 0.0
+    return v
 
 
 def true_residual(dims, U, kappa, b, x, sign=1, antiperiodic=True) -> float:

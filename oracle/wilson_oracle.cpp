@@ -22,6 +22,8 @@
 //   * su(3) algebra gaussian + expand         libraries/datatypes/sun_matrix.h:480-560
 //   * exp() Taylor order 20 (Horner)          libraries/datatypes/matrix.h:3289-3309
 //   * reunitarize = make_unitary + fix_det    libraries/datatypes/sun_matrix.h:137-196
+//   * Wilson force (eo)                       libraries/dirac/wilson.h:110-137, 293-311
+//   * staggered eta, hop, eo apply, force     libraries/dirac/staggered.h:14-86, 224-265
 //
 // Backward hop.  wilson.h:47 (and :92) read vtemp[dir][X + dir] for the
 // backward term, although the U^dagger-multiplied half spinors are stored in
@@ -573,6 +575,113 @@ void or_wilson_eo_force(const int *dims, int tap, const double *U, double kappa,
     std::fill(tmp.begin(), tmp.end(), 0.0);
     or_wilson_hop(dims, tap, U, kappa, psi, tmp.data(), 2, sign, 1);
     calc_force(g, -kappa, chi, tmp.data(), 2, sign, out);
+}
+
+// ---------------------------------------------------------------- staggered
+// Colour-vector fields v[V][3] complex (SU_vector<3,double>), lexicographic.
+
+// staggered_eta[d](x) = ((sum_{d2 < d} x_d2) % 2) * 2 - 1, as staggered.h:14-28
+// computes it (its comment states the opposite sign; the code is followed).
+static inline double stag_eta(const Geom &g, long x, int dir) {
+    int c[4];
+    g.coords(x, c);
+    int s = 0;
+    for (int d2 = 0; d2 < dir; d2++) s += c[d2];
+    return (s % 2) * 2 - 1;
+}
+
+// dirac_staggered_hop, staggered.h:48-68:  for x in par
+//   out(x) += 0.5 sign sum_dir eta_dir(x) [U_dir(x) in(x+dir) - U_dir(x-dir)^dag in(x-dir)]
+// with the fermion boundary sign on the gathered values.
+void or_staggered_hop(const int *dims, int tap, const double *U, const double *in, double *out, int par, int sign) {
+    Geom g(dims, tap);
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        if (!g.in(x, par)) continue;
+        cd acc[3] = {0, 0, 0};
+        for (int dir = 0; dir < 4; dir++) {
+            double sf, sb;
+            const long yf = g.nb(x, dir, +1, &sf), yb = g.nb(x, dir, -1, &sb);
+            const Mat3 uf = load_link(U, g.V, dir, x), ub = load_link(U, g.V, dir, yb);
+            const double eta = stag_eta(g, x, dir);
+            for (int a = 0; a < 3; a++) {
+                cd t = 0;
+                for (int b = 0; b < 3; b++) {
+                    t += uf.e[a][b] * sf * cd(in[6 * yf + 2 * b], in[6 * yf + 2 * b + 1]);
+                    t -= std::conj(ub.e[b][a]) * sb * cd(in[6 * yb + 2 * b], in[6 * yb + 2 * b + 1]);
+                }
+                acc[a] += eta * t;
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            out[6 * x + 2 * a] += 0.5 * sign * acc[a].real();
+            out[6 * x + 2 * a + 1] += 0.5 * sign * acc[a].imag();
+        }
+    }
+}
+
+// dirac_staggered_evenodd::apply / dagger (sign +1 / -1), staggered.h:224-242:
+//   out = 0; out[EVEN] = m in; out[ODD] = (1/m) hop_ODD(in); out[EVEN] += hop_EVEN(out)
+// so out[EVEN] = m in_e + D_eo (1/m) D_oe in_e and out[ODD] keeps (1/m) D_oe in_e.
+void or_staggered_eo_apply(const int *dims, int tap, const double *U, double mass, const double *in, double *out,
+                           int sign) {
+    Geom g(dims, tap);
+    std::memset(out, 0, sizeof(double) * 6 * g.V);
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 1))
+            for (int k = 0; k < 6; k++) out[6 * x + k] = mass * in[6 * x + k];
+    or_staggered_hop(dims, tap, U, in, out, 2, sign);
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 2))
+            for (int k = 0; k < 6; k++) out[6 * x + k] = (1.0 / mass) * out[6 * x + k];
+    std::vector<double> mid(out, out + 6 * g.V);
+    or_staggered_hop(dims, tap, U, mid.data(), out, 1, sign);
+}
+
+// dirac_staggered_calc_force, staggered.h:70-86, accumulated into out[4][V][3][3]:
+//   x in par:      out[dir](x) += -sign 0.5 eta_dir(x) chi(x+dir) (x) psi(x)
+//   x in opp(par): out[dir](x) += sign 0.5 eta_dir(x+dir) psi(x+dir) (x) chi(x)
+// (a (x) b)_ij = a_i conj(b_j), boundary sign on the gathered field.
+static void stag_calc_force(const Geom &g, const double *chi, const double *psi, int sign, int par, double *out) {
+    const int opp = par == 1 ? 2 : 1;
+#pragma omp parallel for schedule(static)
+    for (long x = 0; x < g.V; x++) {
+        const bool in_par = g.in(x, par);
+        if (!in_par && !g.in(x, opp)) continue;
+        for (int dir = 0; dir < 4; dir++) {
+            double sg;
+            const long y = g.nb(x, dir, +1, &sg);
+            const double *a = in_par ? chi : psi, *b = in_par ? psi : chi;
+            const double f = in_par ? -sign * 0.5 * stag_eta(g, x, dir) : sign * 0.5 * stag_eta(g, y, dir);
+            double *o = out + 18 * (dir * g.V + x);
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    const cd v = cd(a[6 * y + 2 * i], a[6 * y + 2 * i + 1]) * sg *
+                                 std::conj(cd(b[6 * x + 2 * j], b[6 * x + 2 * j + 1])) * f;
+                    o[(i * 3 + j) * 2] += v.real();
+                    o[(i * 3 + j) * 2 + 1] += v.imag();
+                }
+        }
+    }
+}
+
+// dirac_staggered_evenodd::force(chi, psi, force, sign), staggered.h:246-265
+void or_staggered_eo_force(const int *dims, int tap, const double *U, double mass, const double *chi,
+                           const double *psi, int sign, double *out) {
+    Geom g(dims, tap);
+    std::memset(out, 0, sizeof(double) * 72 * g.V);
+    std::vector<double> tmp((size_t)6 * g.V, 0.0);
+    or_staggered_hop(dims, tap, U, chi, tmp.data(), 2, -sign);
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 2))
+            for (int k = 0; k < 6; k++) tmp[6 * x + k] *= 1.0 / mass;
+    stag_calc_force(g, tmp.data(), psi, sign, 1, out);
+    std::fill(tmp.begin(), tmp.end(), 0.0);
+    or_staggered_hop(dims, tap, U, psi, tmp.data(), 2, sign);
+    for (long x = 0; x < g.V; x++)
+        if (g.in(x, 2))
+            for (int k = 0; k < 6; k++) tmp[6 * x + k] *= 1.0 / mass;
+    stag_calc_force(g, chi, tmp.data(), sign, 2, out);
 }
 
 // sum over sites of parity par of conj(a) . b  (WilsonVector::dot, conj-linear in a)
