@@ -95,13 +95,17 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
     // d p as an uncontracted product: with d = 1 the sums round exactly as p - k^2 acc
     const float dg = (float)pr.diag;
     auto ds = [dg](Cx<float> v) -> Cx<float> { return {__fmul_rn(dg, v.re), __fmul_rn(dg, v.im)}; };
-    if (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R4L) {
+    if (PHASE == PH_P1 || PHASE == PH_P3) {
         L::sp(pr.t, pr.tn, stride).store(i, acc);
+    } else if (PHASE == PH_R4L) {
+        SpinorF32{reinterpret_cast<float4 *>(pr.t64), stride}.store(i, acc);  // FP32 in the FP64 t buffer
     } else if (PHASE == PH_R5L) {
-        // r = d s - k^2 H^dag t with s_low in Dp (reliable update of M x = b); |r|^2
+        // r = d s - k^2 H^dag t with s in FP32 in y (reliable update of M x = b); |r|^2;
+        // y is cleared again for the solution increments that follow
         const float k2 = (float)(pr.kappa * pr.kappa);
         Spinor<float> sv;
-        L::sp(pr.Dp, pr.Dpn, stride).load_cached(i, sv);
+        SpinorF32 ys{pr.y, stride};
+        ys.load_cached(i, sv);
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
@@ -110,6 +114,10 @@ __device__ __forceinline__ void epi_low(const EngProblem &pr, const EngState &st
             n2 += (double)norm2(v);
         }
         L::sp(pr.r, pr.rn, stride).store(i, acc);
+        Spinor<float> zero;
+#pragma unroll
+        for (int c = 0; c < 12; c++) zero.s[c / 3][c % 3] = {0.f, 0.f};
+        ys.store(i, zero);
         red[0] = n2;
     } else if (PHASE == PH_P2) {
         const float k2 = (float)(pr.kappa * pr.kappa);
@@ -175,12 +183,13 @@ __device__ __forceinline__ void epi_f64(const EngProblem &pr, int stride, int i,
                 const Cx<double> mx = ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3];
                 const Cx<double> bv = ldc(b, stride, c, i);
                 const Cx<double> sv = bv - mx;
-                stc(sp, stride, c, i, sv);
+                // s itself is only read by the FP64 R4 / R5 of the normal system; solve mode
+                // continues from its low-precision copy
                 sl.s[c / 3][c % 3] = {(float)sv.re, (float)sv.im};
                 n2 += norm2(sv);
                 d2 += norm2(bv);
             }
-            Low<LOW>::sp(pr.Dp, pr.Dpn, stride).store(i, sl);  // input of R4L / R5L
+            SpinorF32{pr.y, stride}.store(i, sl);  // input of R4L / R5L (y was cleared by R1)
         } else {
 #pragma unroll
             for (int c = 0; c < 12; c++) stc(sp, stride, c, i, ds(ldc(x, stride, c, i)) - k2 * acc.s[c / 3][c % 3]);
@@ -361,14 +370,20 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
         if (valid && na > 0) nb = site_neighbours(g, i, OUTPAR);
         for (int g0 = 0; g0 < na; g0 += NR) {
             const int cnt = min(NR, na - g0);
-            typename L::Sp in[NR];
+            // the reliable update of M x = b reads FP32 fields: s (in y) and t (in t64)
+            constexpr bool ru32 = PHASE == PH_R4L || PHASE == PH_R5L;
+            using InSp = typename std::conditional<ru32, SpinorF32, typename L::Sp>::type;
+            InSp in[NR];
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 const EngProblem &pr = T->prob[s_act[g0 + min(r, cnt - 1)]];
-                constexpr bool from_dp = PHASE == PH_P3 || PHASE == PH_R4L;
-                void *ip = (PHASE == PH_P1) ? pr.p : (from_dp ? pr.Dp : pr.t);
-                float *inn = (PHASE == PH_P1) ? pr.pn : (from_dp ? pr.Dpn : pr.tn);
-                in[r] = L::sp(ip, inn, stride);
+                if constexpr (ru32) {
+                    in[r] = SpinorF32{PHASE == PH_R4L ? pr.y : reinterpret_cast<float4 *>(pr.t64), stride};
+                } else {
+                    void *ip = (PHASE == PH_P1) ? pr.p : (PHASE == PH_P3 ? pr.Dp : pr.t);
+                    float *inn = (PHASE == PH_P1) ? pr.pn : (PHASE == PH_P3 ? pr.Dpn : pr.tn);
+                    in[r] = L::sp(ip, inn, stride);
+                }
             }
             Spinor<float> acc[NR];
 #pragma unroll
@@ -693,6 +708,8 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 //   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
 //   5: one right-hand side per thread, <= 72 registers (7 blocks)
 //   6: one right-hand side per thread, <= 64 registers (8 blocks)
+//   7: two right-hand sides per thread sharing the links, <= 96 registers (5 blocks)
+//   8: three right-hand sides per thread sharing the links, <= 128 registers (4 blocks)
 // variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
@@ -715,6 +732,12 @@ void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, con
         break;
     case 6:
         enqueue_iteration_t<LOW, 1, 8, FULL18>(P, G, s, ev);
+        break;
+    case 7:
+        enqueue_iteration_t<LOW, 2, 5, FULL18>(P, G, s, ev);
+        break;
+    case 8:
+        enqueue_iteration_t<LOW, 3, 4, FULL18>(P, G, s, ev);
         break;
     default:
         enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s, ev);
@@ -777,6 +800,10 @@ int occupancy_variant(int v) {
         return occupancy_low<LOW, 1, 7>();
     case 6:
         return occupancy_low<LOW, 1, 8>();
+    case 7:
+        return occupancy_low<LOW, 2, 5>();
+    case 8:
+        return occupancy_low<LOW, 3, 4>();
     default:
         return occupancy_low<LOW, 1, 4>();
     }

@@ -18,12 +18,12 @@
 // Reliable update (FP64, only slots that asked for it):
 //   R1  x += y; y = 0                          (FP64 solution accumulation)
 //   R2  t64 = H^{oe}_+ x
-//   R3  solve mode:  s = b - (x - kappa^2 H t64)   |s|^2, |b|^2; s also in low precision (Dp)
-//       normal mode: s = x - kappa^2 H t64         (= M x)
+//   R3  solve mode:  s = b - (x - kappa^2 H t64)   |s|^2, |b|^2; s kept in FP32 (in y)
+//       normal mode: s = x - kappa^2 H t64         (= M x, FP64)
 //   R4  normal mode: t64 = H^{oe}_- s
-//   R4L solve mode:  t = H^{oe}_- s_low            (low precision)
+//   R4L solve mode:  t = H^{oe}_- s               (FP32, in the t64 buffer; low-precision links)
 //   R5  normal mode: r = b - (s - kappa^2 H^dag t64) (= b - M^dag M x), |b|^2
-//   R5L solve mode:  r = s_low - kappa^2 H^dag t    (= M^dag (b - M x), low precision)
+//   R5L solve mode:  r = s - kappa^2 H^dag t       (= M^dag (b - M x), FP32); y cleared
 //       r_low = r, |r|^2 -> true residual, convergence, beta
 //   P5  p = r + beta p   (p = r on a slot's first iteration)
 #pragma once
@@ -122,8 +122,8 @@ struct EngGrid {
 };
 
 // in launch order; R4 / R5 serve slots of the normal system (FP64), R4L / R5L those of
-// M x = b (low precision: r = M^dag s only feeds the low-precision iteration, and s
-// = b - M x, on which convergence is decided, stays FP64)
+// M x = b (FP32: r = M^dag s only feeds the low-precision iteration, and s = b - M x,
+// on which convergence is decided, is formed and measured in FP64)
 enum EngPhase : int {
     PH_P1 = 0, PH_P2, PH_P3, PH_P4, PH_R1, PH_R2, PH_R3, PH_R4, PH_R4L, PH_R5, PH_R5L, PH_P5
 };

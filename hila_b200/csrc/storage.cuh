@@ -388,6 +388,7 @@ __device__ __forceinline__ void hop_dir_multi(const SiteNbrs &n, int par, int i,
                                               const Lk &U, Spinor<R> (&acc)[NR]) {
     Cx<R> h0[3], h1[3], v0[3], v1[3];
     Su3<R> u;
+    // one colour-multiplied half spinor live at a time (expand_add_scaled_half)
     U.load(par, MU, i, u);
 #pragma unroll
     for (int r = 0; r < NR; r++) {
@@ -396,8 +397,9 @@ __device__ __forceinline__ void hop_dir_multi(const SiteNbrs &n, int par, int i,
             in[r].template load_proj<MU, SIGN>(n.fwd[MU], h0, h1, sc);
             if (MU == 3 && n.tfwd_wrap) sc = -sc;
             su3_mul(u, h0, v0);
+            expand_add_scaled_half<MU, SIGN, 0>(acc[r], v0, sc);
             su3_mul(u, h1, v1);
-            expand_add_scaled<MU, SIGN>(acc[r], v0, v1, sc);
+            expand_add_scaled_half<MU, SIGN, 1>(acc[r], v1, sc);
         }
     }
     U.load(1 - par, MU, n.bwd[MU], u);
@@ -408,8 +410,9 @@ __device__ __forceinline__ void hop_dir_multi(const SiteNbrs &n, int par, int i,
             in[r].template load_proj<MU, -SIGN>(n.bwd[MU], h0, h1, sc);
             if (MU == 3 && n.tbwd_wrap) sc = -sc;
             su3_adj_mul(u, h0, v0);
+            expand_add_scaled_half<MU, -SIGN, 0>(acc[r], v0, sc);
             su3_adj_mul(u, h1, v1);
-            expand_add_scaled<MU, -SIGN>(acc[r], v0, v1, sc);
+            expand_add_scaled_half<MU, -SIGN, 1>(acc[r], v1, sc);
         }
     }
 }
@@ -461,10 +464,10 @@ __device__ __forceinline__ void hop_site(const Geom &g, int par, int i, const Sp
 #pragma unroll
     for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {R(0), R(0)};
     SiteNbrs n = site_neighbours(g, i, par);
-    hop_dir<0, SIGN>(n, par, i, in, U, acc);
-    hop_dir<1, SIGN>(n, par, i, in, U, acc);
-    hop_dir<2, SIGN>(n, par, i, in, U, acc);
-    hop_dir<3, SIGN>(n, par, i, in, U, acc);
+    hop_dir_lean<0, SIGN>(n, par, i, in, U, acc);
+    hop_dir_lean<1, SIGN>(n, par, i, in, U, acc);
+    hop_dir_lean<2, SIGN>(n, par, i, in, U, acc);
+    hop_dir_lean<3, SIGN>(n, par, i, in, U, acc);
 }
 
 }  // namespace hw

@@ -278,6 +278,32 @@ __device__ __forceinline__ void expand_add_scaled(Spinor<R> &acc, const Cx<R> h0
     }
 }
 
+// expand_add_scaled for one projected component (Q = 0: h0, Q = 1: h1); the pair
+// for Q = 0 and 1 equals expand_add_scaled element by element
+template <int DIR, int SIGN, int Q, typename R>
+__device__ __forceinline__ void expand_add_scaled_half(Spinor<R> &acc, const Cx<R> h[3], R sc) {
+    const R sp = SIGN > 0 ? sc : -sc;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        acc.s[Q][k] = axpy(acc.s[Q][k], sc, h[k]);
+        if (DIR == 0) {  // r2 = -s i h1, r3 = -s i h0
+            acc.s[Q == 0 ? 3 : 2][k] = axpy_i(acc.s[Q == 0 ? 3 : 2][k], -sp, h[k]);
+        } else if (DIR == 1) {  // r2 = s h1, r3 = -s h0
+            if (Q == 0)
+                acc.s[3][k] = axpy(acc.s[3][k], -sp, h[k]);
+            else
+                acc.s[2][k] = axpy(acc.s[2][k], sp, h[k]);
+        } else if (DIR == 2) {  // r2 = -s i h0, r3 = s i h1
+            if (Q == 0)
+                acc.s[2][k] = axpy_i(acc.s[2][k], -sp, h[k]);
+            else
+                acc.s[3][k] = axpy_i(acc.s[3][k], sp, h[k]);
+        } else {  // r2 = s h0, r3 = s h1
+            acc.s[Q == 0 ? 2 : 3][k] = axpy(acc.s[Q == 0 ? 2 : 3][k], sp, h[k]);
+        }
+    }
+}
+
 // ----------------------------------------------------------------- geometry
 //
 // Even-odd layout: a site with lexicographic index
