@@ -374,7 +374,7 @@ int Engine::configure() {
     int variant = default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
     // the tensor-core variant reads the 18-real FP16 links, which exist only with full18_
-    if (variant < 0 || variant > 8 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
+    if (variant < 0 || variant > 7 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
     if (variant != grid_.variant || mask != grid_.planes_mask) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
         if (chunk_exec_) {

@@ -11,6 +11,7 @@
 #include <type_traits>
 
 #include "engine.h"
+#include "pair.cuh"
 #include "reduce.cuh"
 #include "storage.cuh"
 
@@ -333,8 +334,9 @@ __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLat
 
 // Inner phases P1..P4 in low precision.  Each thread owns one site and up to
 // NR right-hand sides at a time, so links, their third rows and the neighbour
-// indices are shared by the NR solves.
-template <int PHASE, int LOW, int NR, int MINB, bool FULL18>
+// indices are shared by the NR solves.  PK (with NR = 2 and FP16 input): the two
+// solves run in the two lanes of packed FP32 instructions (pair.cuh).
+template <int PHASE, int LOW, int NR, int MINB, bool FULL18, bool PK = false>
 __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
     constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2) ? 1 : -1;
     constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3 || PHASE == PH_R4L) ? 1 : 0;
@@ -392,10 +394,27 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
                 for (int c = 0; c < 12; c++) acc[r].s[c / 3][c % 3] = {0.f, 0.f};
             if (valid) {
                 const typename InnerLinks<LOW, FULL18>::Lk U = InnerLinks<LOW, FULL18>::lk(La);
-                hop_dir_multi<0, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
-                hop_dir_multi<1, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
-                hop_dir_multi<2, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
-                hop_dir_multi<3, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                if constexpr (PK && NR == 2 && std::is_same<InSp, SpinorF16>::value) {
+                    // a lone last solve fills both lanes (in[1] repeats in[0]); lane y is dropped
+                    Spinor2 a2;
+#pragma unroll
+                    for (int c = 0; c < 12; c++) a2.s[c / 3][c % 3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+                    hop_dir_pair<0, SIGN>(nb, OUTPAR, i, in[0], in[1], U, a2);
+                    hop_dir_pair<1, SIGN>(nb, OUTPAR, i, in[0], in[1], U, a2);
+                    hop_dir_pair<2, SIGN>(nb, OUTPAR, i, in[0], in[1], U, a2);
+                    hop_dir_pair<3, SIGN>(nb, OUTPAR, i, in[0], in[1], U, a2);
+#pragma unroll
+                    for (int c = 0; c < 12; c++) {
+                        const Cx2 v = a2.s[c / 3][c % 3];
+                        acc[0].s[c / 3][c % 3] = {v.re.x, v.im.x};
+                        acc[NR - 1].s[c / 3][c % 3] = {v.re.y, v.im.y};
+                    }
+                } else {
+                    hop_dir_multi<0, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                    hop_dir_multi<1, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                    hop_dir_multi<2, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                    hop_dir_multi<3, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
+                }
             }
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -662,26 +681,42 @@ void enqueue_reliable_update(const EngPtrs &P, const EngGrid &G, cudaStream_t s,
     mark(ev, kEngPhases, s);
 }
 
-template <int LOW, int NR, int MINB, bool FULL18>
+template <int LOW, int NR, int MINB, bool FULL18, bool PK = false>
 struct LowShape {
     template <int PHASE>
     static void launch(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
-        k_eng_low<PHASE, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+        k_eng_low<PHASE, LOW, NR, MINB, FULL18, PK><<<G.low, kEngTile, 0, s>>>(P);
     }
 };
 
-template <int LOW, int NR, int MINB, bool FULL18>
+template <int LOW, int NR, int MINB, bool FULL18, bool PK = false>
 void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     mark(ev, 0, s);
-    k_eng_low<PH_P1, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P1, LOW, NR, MINB, FULL18, PK><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 1, s);
-    k_eng_low<PH_P2, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P2, LOW, NR, MINB, FULL18, PK><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 2, s);
-    k_eng_low<PH_P3, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P3, LOW, NR, MINB, FULL18, PK><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 3, s);
-    k_eng_low<PH_P4, LOW, NR, MINB, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P4, LOW, NR, MINB, FULL18, PK><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 4, s);
-    enqueue_reliable_update<LOW, LowShape<LOW, NR, MINB, FULL18>>(P, G, s, ev);
+    enqueue_reliable_update<LOW, LowShape<LOW, NR, MINB, FULL18, PK>>(P, G, s, ev);
+}
+
+// P1..P3 with two solves per thread in packed FP32 (MINB_PK blocks per SM, G.pk
+// blocks), P4 and the reliable update in the shape of variant 2 (G.low blocks)
+template <int LOW, int MINB_PK, bool FULL18>
+void enqueue_iteration_hybrid(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
+    mark(ev, 0, s);
+    k_eng_low<PH_P1, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
+    mark(ev, 1, s);
+    k_eng_low<PH_P2, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
+    mark(ev, 2, s);
+    k_eng_low<PH_P3, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
+    mark(ev, 3, s);
+    k_eng_low<PH_P4, LOW, 1, 6, FULL18><<<G.low, kEngTile, 0, s>>>(P);
+    mark(ev, 4, s);
+    enqueue_reliable_update<LOW, LowShape<LOW, 1, 6, FULL18>>(P, G, s, ev);
 }
 
 constexpr int kMmaMinBlocks = 4;
@@ -706,10 +741,10 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 //   2: one right-hand side per thread, <= 85 registers (6 blocks)
 //   3: two right-hand sides per thread sharing the links, <= 128 registers
 //   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
-//   5: one right-hand side per thread, <= 72 registers (7 blocks)
-//   6: one right-hand side per thread, <= 64 registers (8 blocks)
-//   7: two right-hand sides per thread sharing the links, <= 96 registers (5 blocks)
-//   8: three right-hand sides per thread sharing the links, <= 128 registers (4 blocks)
+//   5: FP16: two right-hand sides per thread in the lanes of packed FP32
+//      instructions (pair.cuh), <= 128 registers, every inner phase
+//   6, 7: P1..P3 packed as in 5 with <= 128 / 168 registers (4 / 3 blocks), P4 and the
+//      reliable update as variant 2 (FP32 input falls back to variant 3's hop)
 // variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
@@ -728,16 +763,13 @@ void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, con
         enqueue_iteration_t<LOW, 2, 4, FULL18>(P, G, s, ev);
         break;
     case 5:
-        enqueue_iteration_t<LOW, 1, 7, FULL18>(P, G, s, ev);
+        enqueue_iteration_t<LOW, 2, 4, FULL18, true>(P, G, s, ev);
         break;
     case 6:
-        enqueue_iteration_t<LOW, 1, 8, FULL18>(P, G, s, ev);
+        enqueue_iteration_hybrid<LOW, 4, FULL18>(P, G, s, ev);
         break;
     case 7:
-        enqueue_iteration_t<LOW, 2, 5, FULL18>(P, G, s, ev);
-        break;
-    case 8:
-        enqueue_iteration_t<LOW, 3, 4, FULL18>(P, G, s, ev);
+        enqueue_iteration_hybrid<LOW, 3, FULL18>(P, G, s, ev);
         break;
     default:
         enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s, ev);
@@ -775,10 +807,10 @@ void eng_convert_links(const Geom &g, const double2 *l64, int planes, int stride
     k_eng_links<<<grid, 256, 0, s>>>(g, l64, planes, stride, l32, l16a, l16b, l32a, l32b, l16x, l16z);
 }
 
-template <int LOW, int NR, int MINB>
+template <int LOW, int NR, int MINB, bool PK = false, int PHASE = PH_P4>
 int occupancy_low() {
     int lo = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_low<PH_P4, LOW, NR, MINB, true>, kEngTile, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, k_eng_low<PHASE, LOW, NR, MINB, true, PK>, kEngTile, 0);
     return lo < 1 ? 1 : lo;
 }
 
@@ -793,17 +825,13 @@ int occupancy_variant(int v) {
     case 1:
         return occupancy_low<LOW, 1, 5>();
     case 2:
+    case 6:
+    case 7:
         return occupancy_low<LOW, 1, 6>();
     case 3:
         return occupancy_low<LOW, 2, 4>();
     case 5:
-        return occupancy_low<LOW, 1, 7>();
-    case 6:
-        return occupancy_low<LOW, 1, 8>();
-    case 7:
-        return occupancy_low<LOW, 2, 5>();
-    case 8:
-        return occupancy_low<LOW, 3, 4>();
+        return occupancy_low<LOW, 2, 4, true>();
     default:
         return occupancy_low<LOW, 1, 4>();
     }
@@ -817,6 +845,14 @@ EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hi, k_eng_f64<PH_R5, LOW_F32, 9>, kEngTile, 0);
     EngGrid G;
     G.low = sms * lo;
+    G.pk = G.low;
+    if (variant == 6 || variant == 7) {
+        const int pk = low == LOW_F16 ? (variant == 6 ? occupancy_low<LOW_F16, 2, 4, true, PH_P1>()
+                                                       : occupancy_low<LOW_F16, 2, 3, true, PH_P1>())
+                                      : (variant == 6 ? occupancy_low<LOW_F32, 2, 4, true, PH_P1>()
+                                                       : occupancy_low<LOW_F32, 2, 3, true, PH_P1>());
+        G.pk = sms * pk;
+    }
     G.f64 = sms * (hi < 1 ? 1 : hi);
     G.variant = variant;
     G.full18 = full18;

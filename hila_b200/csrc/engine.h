@@ -116,6 +116,7 @@ struct EngPtrs {
 struct EngGrid {
     int low;  // blocks of the low-precision phases (all SMs x resident blocks)
     int f64;  // blocks of the FP64 reliable-update phases
+    int pk;   // blocks of the packed two-solve phases of the hybrid shapes (engine.cu)
     int variant;  // launch shape of the low-precision phases (engine.cu)
     int full18;   // 1: inner phases read 18-real links (FP32 or FP16); 0: the 12-real links of the precision
     int planes_mask;  // FP64 link formats present: bit 0 = 18 reals, bit 1 = 12 reals

@@ -96,7 +96,8 @@ class Engine {
     bool use_graph_ = true;
     bool full18_ = false;
     // launch shape of the inner phases (engine.cu): one RHS per thread, 6 blocks per SM
-    int default_variant() const { return 2; }
+    // FP16: packed two-solve P1..P3 (fastest measured); FP32: one solve per thread
+    int default_variant() const { return low_ == LOW_F16 ? 7 : 2; }
 };
 
 // per-context engine for a low precision (LOW_F32 / LOW_F16), created on first use
