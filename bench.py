@@ -65,6 +65,11 @@ ITERS_PER_SOLVE = {"cg": 59, "mrhs": 59, "cg8": None}
 # capture at 24^4; every array is read once, so it scales with the sites.
 P4_TRAFFIC_PER_SITE_12 = 999.2e6 / 165888
 
+# DRAM traffic of the two k_hop launches of one even-odd apply (12-real FP64 links), per
+# output site, from one ncu capture at 32^4 (524,288 sites): every array is read once, so
+# it scales with the sites.  None until a capture of the current kernels is recorded.
+HOP_F64_12_TRAFFIC_PER_SITE = None
+
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -227,7 +232,7 @@ def run_ours(args, dist: Dist):
     link_bytes = 144 if args.link_format == 18 else 96
     # algorithmic bytes per hop launch (one output site): 8 links + neighbour spinors once + output
     hop_bytes = 8 * link_bytes + 192 + 192
-    apply_bytes = (2 * hop_bytes + 192) * Vh  # second hop also reads in_e
+    apply_bytes = (2 * hop_bytes + 2 * 192) * Vh  # second hop also reads in_e and clears out_o
 
     def dslash_time(nrep):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -398,9 +403,13 @@ def run_ours(args, dist: Dist):
         result["dslash_ms_per_apply"] = roof_ms
     hop_ms = roof_ms / 2
     achieved = (apply_bytes / 2) / (hop_ms * 1e-3) / 1e9
+    hop_traffic = None
+    if args.link_format == 12 and HOP_F64_12_TRAFFIC_PER_SITE:
+        hop_traffic = {"bytes_per_launch": int(HOP_F64_12_TRAFFIC_PER_SITE * Vh / 2),
+                       "source": "ncu capture at 32^4 (mean of the apply's two launches) scaled by sites"}
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "traffic": None, "kernel": "k_hop (FP64, %d-real links)" % args.link_format,
+                "traffic": hop_traffic, "kernel": "k_hop (FP64, %d-real links)" % args.link_format,
                 "algorithmic_bytes_per_launch": apply_bytes / 2}
     if args.workload == "mrhs":
         # the dominant kernel of the batched solve: the engine's P4 phase

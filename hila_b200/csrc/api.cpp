@@ -357,11 +357,11 @@ static int eo_apply(const hw_gauge *G, double kappa, const hw_field *in, hw_fiel
     if ((rc = ensure_workspace(lat)) != HW_OK) return rc;
     if ((rc = tune_hop(lat, G)) != HW_OK) return rc;
     CgWorkspace &w = *lat->ws;
-    // t_o = H^{oe}_s in_e ; out_e = in_e - kappa^2 H^{eo}_s t_o ; out_o = 0  (wilson.h:272-279)
+    // t_o = H^{oe}_s in_e ; out_e = in_e - kappa^2 H^{eo}_s t_o ; out_o = 0  (wilson.h:272-279);
+    // the second hop clears out_o as it goes (the odd half of `in` is not read)
     launch_hop_scale(lat->g, G->U(), 1, sign, in->half[0].h(), w.t.h(), 1.0, nullptr, ctx->stream);
     launch_hop_xpay(lat->g, G->U(), 0, sign, w.t.h(), in->half[0].h(), out->half[0].h(), -kappa * kappa, nullptr,
-                    nullptr, ctx->stream, d);
-    HW_CUDA(cudaMemsetAsync(out->half[1].buf.ptr, 0, out->half[1].buf.bytes, ctx->stream));
+                    nullptr, ctx->stream, d, out->half[1].buf.as<double2>());
     // stream-ordered: later calls on this context see the result; downloads synchronise
     HW_CUDA(cudaGetLastError());
     return HW_OK;

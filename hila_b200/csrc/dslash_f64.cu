@@ -19,9 +19,22 @@ namespace {
 
 __host__ __device__ __forceinline__ SpinorF64 sp(HalfF64 h) { return SpinorF64{h.p, h.stride}; }
 
+// Epilogue operands read at the output site (not at neighbours) are copied into
+// shared memory with cp.async when the thread starts, so their HBM reads overlap
+// the hop instead of following it.  An epilogue with NPRE > 0 names them in
+// pre(k) and reads them from stg (component c of operand k at stg.p[(k*12 + c)
+// * BLOCK + threadIdx.x]; `stg.stride` = BLOCK, index ix = threadIdx.x).
+// (cp_async16 and cp_async_wait_all: storage.cuh)
+// operand k of a staged epilogue as a field over the block's threads
+__device__ __forceinline__ SpinorF64 staged(double2 *stage, int block, int k) {
+    return SpinorF64{stage + (size_t)k * 12 * block, block};
+}
+
 // out = a * H in
 struct EpiScale {
     static constexpr int NRED = 0;
+    static constexpr int NPRE = 0;
+    __device__ SpinorF64 pre(int) const { return out; }
     SpinorF64 out;
     double a;
     const CgState *st;
@@ -51,19 +64,27 @@ __device__ __forceinline__ Cx<double> dscale(double d, Cx<double> v) { return {_
 template <bool RED>
 struct EpiXpay {
     static constexpr int NRED = RED ? 1 : 0;
+    static constexpr int NPRE = 1;  // x
     SpinorF64 x, out;
     double b;
     CgState *st;
     double d;
+    double2 *zero;  // optional: cleared at site i (stride of out)
+    __device__ SpinorF64 pre(int) const { return x; }
     __device__ bool skip() const { return st && st->status != CG_RUNNING; }
-    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+    __device__ void operator()(int i, Spinor<double> &acc, double *red, double2 *stage, int block) const {
+        const SpinorF64 xs = staged(stage, block, 0);
+        const int ix = threadIdx.x;
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> v = dscale(d, load_c(x, c, i)) + b * acc.s[c / 3][c % 3];
+            Cx<double> v = dscale(d, load_c(xs, c, ix)) + b * acc.s[c / 3][c % 3];
             store_c(out, c, i, v);
             n2 += norm2(v);
         }
+        if (zero)
+#pragma unroll
+            for (int c = 0; c < 12; c++) zero[(size_t)c * out.stride + i] = make_double2(0.0, 0.0);
         if (RED) red[0] = n2;
     }
     __device__ void operator()(const double *tot) {
@@ -81,18 +102,22 @@ struct EpiXpay {
 // DDp = d Dp + b H t ; x += alpha p ; r -= alpha DDp ; rrnew = |r|^2
 struct EpiCgUpdate {
     static constexpr int NRED = 1;
+    static constexpr int NPRE = 2;  // Dp, r
     SpinorF64 Dp, r, x, p;
     double b;
     CgState *st;
     double d;
+    __device__ SpinorF64 pre(int k) const { return k == 0 ? Dp : r; }
     __device__ bool skip() const { return st->status != CG_RUNNING; }
-    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+    __device__ void operator()(int i, Spinor<double> &acc, double *red, double2 *stage, int block) const {
+        const SpinorF64 ds = staged(stage, block, 0), rs = staged(stage, block, 1);
+        const int ix = threadIdx.x;
         const double alpha = st->alpha;
         double n2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> ddp = dscale(d, load_c(Dp, c, i)) + b * acc.s[c / 3][c % 3];
-            Cx<double> rv = load_c(r, c, i) - alpha * ddp;
+            Cx<double> ddp = dscale(d, load_c(ds, c, ix)) + b * acc.s[c / 3][c % 3];
+            Cx<double> rv = load_c(rs, c, ix) - alpha * ddp;
             store_c(r, c, i, rv);
             store_c(x, c, i, load_c(x, c, i) + alpha * load_c(p, c, i));
             n2 += norm2(rv);
@@ -119,17 +144,21 @@ struct EpiCgUpdate {
 // res = src - (d x + b H t) ; |res|^2, |src|^2
 struct EpiResidual {
     static constexpr int NRED = 2;
+    static constexpr int NPRE = 2;  // x, src
     SpinorF64 x, src, res;
     double b;
     CgState *st;
     double d;
+    __device__ SpinorF64 pre(int k) const { return k == 0 ? x : src; }
     __device__ bool skip() const { return false; }
-    __device__ void operator()(int i, Spinor<double> &acc, double *red) const {
+    __device__ void operator()(int i, Spinor<double> &acc, double *red, double2 *stage, int block) const {
+        const SpinorF64 xs = staged(stage, block, 0), ss = staged(stage, block, 1);
+        const int ix = threadIdx.x;
         double n2 = 0, d2 = 0;
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            Cx<double> sv = load_c(src, c, i);
-            Cx<double> v = sv - (dscale(d, load_c(x, c, i)) + b * acc.s[c / 3][c % 3]);
+            Cx<double> sv = load_c(ss, c, ix);
+            Cx<double> v = sv - (dscale(d, load_c(xs, c, ix)) + b * acc.s[c / 3][c % 3]);
             if (res.p) store_c(res, c, i, v);
             n2 += norm2(v);
             d2 += norm2(sv);
@@ -145,17 +174,48 @@ struct EpiResidual {
 
 template <int SIGN, int BLOCK, int MINB, class Lk, class Epi>
 __global__ void __launch_bounds__(BLOCK, MINB) k_hop(Geom g, Lk U, int par, SpinorF64 in, Epi epi, RedBuf red) {
+    extern __shared__ double2 stage[];  // Epi::NPRE x 12 x BLOCK
     if (epi.skip()) return;
     const int i = blockIdx.x * BLOCK + threadIdx.x;
     double v[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
     for (int k = 0; k < (Epi::NRED > 0 ? Epi::NRED : 1); k++) v[k] = 0.0;
     if (i < g.Vh) {
+        if constexpr (Epi::NPRE > 0) {
+#pragma unroll
+            for (int k = 0; k < Epi::NPRE; k++) {
+                const SpinorF64 f = epi.pre(k);
+#pragma unroll
+                for (int c = 0; c < 12; c++)
+                    cp_async16(stage + ((size_t)k * 12 + c) * BLOCK + threadIdx.x, f.p + (size_t)c * f.stride + i);
+            }
+        }
         Spinor<double> acc;
         hop_site<SIGN>(g, par, i, in, U, acc);
-        epi(i, acc, v);
+        if constexpr (Epi::NPRE > 0) {
+            cp_async_wait_all();  // this thread's own copies: no block barrier needed
+            epi(i, acc, v, stage, BLOCK);
+        } else {
+            epi(i, acc, v);
+        }
     }
     if constexpr (Epi::NRED > 0) grid_reduce<Epi::NRED, BLOCK>(v, red.partials, red.ticket, epi);
+}
+
+// shared memory of the staged epilogue operands; near the 48 KB default the kernel
+// is opted in once (per instantiation)
+template <int SIGN, int BLOCK, int MINB, class Lk, class Epi>
+size_t hop_smem() {
+    constexpr size_t bytes = (size_t)Epi::NPRE * 12 * BLOCK * sizeof(double2);
+    if constexpr (bytes > 32 * 1024) {
+        static const bool once = [] {
+            cudaFuncSetAttribute(k_hop<SIGN, BLOCK, MINB, Lk, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes);
+            return true;
+        }();
+        (void)once;
+    }
+    return bytes;
 }
 
 template <int BLOCK, int MINB, class Lk, class Epi>
@@ -163,9 +223,9 @@ void launch_variant(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin
                     cudaStream_t s) {
     dim3 grid((g.Vh + BLOCK - 1) / BLOCK);
     if (sign > 0)
-        k_hop<1, BLOCK, MINB><<<grid, BLOCK, 0, s>>>(g, L, par, sin, epi, rb);
+        k_hop<1, BLOCK, MINB><<<grid, BLOCK, hop_smem<1, BLOCK, MINB, Lk, Epi>(), s>>>(g, L, par, sin, epi, rb);
     else
-        k_hop<-1, BLOCK, MINB><<<grid, BLOCK, 0, s>>>(g, L, par, sin, epi, rb);
+        k_hop<-1, BLOCK, MINB><<<grid, BLOCK, hop_smem<-1, BLOCK, MINB, Lk, Epi>(), s>>>(g, L, par, sin, epi, rb);
 }
 
 // Launch shapes the autotuner chooses from (HopVariant in kernels.h):
@@ -362,12 +422,12 @@ void launch_hop_scale(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF
 }
 
 void launch_hop_xpay(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 x, HalfF64 out,
-                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d) {
+                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d, double2 *zero) {
     if (red) {
-        EpiXpay<true> e{sp(x), sp(out), b, st, d};
+        EpiXpay<true> e{sp(x), sp(out), b, st, d, zero};
         dispatch_hop(g, U, par, sign, in, e, red, s);
     } else {
-        EpiXpay<false> e{sp(x), sp(out), b, st, d};
+        EpiXpay<false> e{sp(x), sp(out), b, st, d, zero};
         dispatch_hop(g, U, par, sign, in, e, nullptr, s);
     }
 }

@@ -343,10 +343,16 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
     constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4 || PHASE == PH_R5L) ? 1 : 0;
     using L = Low<LOW>;
     if (eng_ru_phase(PHASE) && *(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
+    // 18-real FP16 links: a site's eight links are copied into shared memory once per
+    // tile and read from there by each of its right-hand sides.  Not in P4 and R5L,
+    // whose epilogues need the resident blocks the 36 KB would cost (measured slower).
+    constexpr bool STAGE = LOW == LOW_F16 && FULL18 && PHASE != PH_P4 && PHASE != PH_R5L;
     __shared__ double smem[kEngTile / 32];
     __shared__ bool last;
     __shared__ int s_act[kEngMaxRhs];
     __shared__ int s_na;
+    __shared__ uint4 s_lx[STAGE ? 16 * kEngTile : 1];
+    __shared__ unsigned s_lz[STAGE ? 8 * kEngTile : 1];
     const EngTables *T = P.T;
     const int ntiles = T->ntiles;
     const int max_tiles = T->max_tiles;
@@ -370,6 +376,13 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
         const int na = s_na;
         SiteNbrs nb;
         if (valid && na > 0) nb = site_neighbours(g, i, OUTPAR);
+        const LinksF16x18Smem<kEngTile> US{s_lx, s_lz, OUTPAR};
+        if constexpr (STAGE) {
+            if (valid && na > 0) {
+                US.stage(InnerLinks<LOW, FULL18>::lk(La), nb, i);
+                cp_async_wait_all();
+            }
+        }
         for (int g0 = 0; g0 < na; g0 += NR) {
             const int cnt = min(NR, na - g0);
             // the reliable update of M x = b reads FP32 fields: s (in y) and t (in t64)
@@ -393,7 +406,14 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
 #pragma unroll
                 for (int c = 0; c < 12; c++) acc[r].s[c / 3][c % 3] = {0.f, 0.f};
             if (valid) {
-                const typename InnerLinks<LOW, FULL18>::Lk U = InnerLinks<LOW, FULL18>::lk(La);
+                using Lk = typename std::conditional<STAGE, LinksF16x18Smem<kEngTile>,
+                                                     typename InnerLinks<LOW, FULL18>::Lk>::type;
+                const Lk U = [&]() -> Lk {
+                    if constexpr (STAGE)
+                        return US;
+                    else
+                        return InnerLinks<LOW, FULL18>::lk(La);
+                }();
                 if constexpr (PK && NR == 2 && std::is_same<InSp, SpinorF16>::value) {
                     // a lone last solve fills both lanes (in[1] repeats in[0]); lane y is dropped
                     Spinor2 a2;
@@ -703,14 +723,14 @@ void enqueue_iteration_t(const EngPtrs &P, const EngGrid &G, cudaStream_t s, con
     enqueue_reliable_update<LOW, LowShape<LOW, NR, MINB, FULL18, PK>>(P, G, s, ev);
 }
 
-// P1..P3 with two solves per thread in packed FP32 (MINB_PK blocks per SM, G.pk
-// blocks), P4 and the reliable update in the shape of variant 2 (G.low blocks)
+// P1 and P3 with two solves per thread in packed FP32 (MINB_PK blocks per SM, G.pk
+// blocks), P2, P4 and the reliable update in the shape of variant 2 (G.low blocks)
 template <int LOW, int MINB_PK, bool FULL18>
 void enqueue_iteration_hybrid(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     mark(ev, 0, s);
     k_eng_low<PH_P1, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
     mark(ev, 1, s);
-    k_eng_low<PH_P2, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
+    k_eng_low<PH_P2, LOW, 1, 6, FULL18><<<G.low, kEngTile, 0, s>>>(P);
     mark(ev, 2, s);
     k_eng_low<PH_P3, LOW, 2, MINB_PK, FULL18, true><<<G.pk, kEngTile, 0, s>>>(P);
     mark(ev, 3, s);
@@ -743,8 +763,8 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 //   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
 //   5: FP16: two right-hand sides per thread in the lanes of packed FP32
 //      instructions (pair.cuh), <= 128 registers, every inner phase
-//   6, 7: P1..P3 packed as in 5 with <= 128 / 168 registers (4 / 3 blocks), P4 and the
-//      reliable update as variant 2 (FP32 input falls back to variant 3's hop)
+//   6, 7: P1, P3 packed as in 5 with <= 128 / 168 registers (4 / 3 blocks), P2, P4 and
+//      the reliable update as variant 2 (FP32 input falls back to variant 3's hop)
 // variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {

@@ -54,9 +54,12 @@ void launch_hop_scale(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF
                       const CgState *st, cudaStream_t s);
 // The x-type term of the epilogues below carries a factor d (1 + m_h for the
 // Hasenbusch operator M + m_h, Hasenbusch.h:16-52; 1 for M itself).
-// out = d x + b * H_s in; with red != null also |out|^2 -> st->pAp and alpha = rr/pAp
+// out = d x + b * H_s in; with red != null also |out|^2 -> st->pAp and alpha = rr/pAp.
+// zero (optional): a half-lattice field on out's sites (the other parity of out) that
+// the same launch clears, site i by the thread of output site i.
 void launch_hop_xpay(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 in, HalfF64 x, HalfF64 out,
-                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d = 1.0);
+                     double b, CgState *st, const RedBuf *red, cudaStream_t s, double d = 1.0,
+                     double2 *zero = nullptr);
 // CG update fused into the last hop of M^dagger M p:
 //   DDp = d Dp + b * H_s t;  r -= alpha DDp;  x += alpha p;  |r|^2 -> st (beta, status)
 void launch_hop_cg_update(const Geom &g, const GaugeF64 &U, int par, int sign, HalfF64 t, HalfF64 Dp,

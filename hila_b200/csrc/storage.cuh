@@ -316,12 +316,7 @@ struct LinksF16x18 {
     const uint4 *p;      // 2 planes per (parity, dir)
     const unsigned *q;   // 1 plane per (parity, dir)
     int stride;
-    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
-        const int pd = par * 4 + dir;
-        uint4 a[2];
-        a[0] = __ldg(p + (size_t)(2 * pd) * stride + i);
-        a[1] = __ldg(p + (size_t)(2 * pd + 1) * stride + i);
-        unsigned b = __ldg(q + (size_t)pd * stride + i);
+    static __device__ __forceinline__ void unpack(const uint4 (&a)[2], unsigned b, Su3<float> &u) {
         const __half2 *ha = reinterpret_cast<const __half2 *>(a);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
@@ -330,6 +325,55 @@ struct LinksF16x18 {
         }
         float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&b));
         u.e[2][2] = {f.x, f.y};
+    }
+    __device__ __forceinline__ void load(int par, int dir, int i, Su3<float> &u) const {
+        const int pd = par * 4 + dir;
+        uint4 a[2];
+        a[0] = __ldg(p + (size_t)(2 * pd) * stride + i);
+        a[1] = __ldg(p + (size_t)(2 * pd + 1) * stride + i);
+        unpack(a, __ldg(q + (size_t)pd * stride + i), u);
+    }
+};
+
+// cp.async (per-thread asynchronous global -> shared copies; a thread that reads
+// only what it copied itself needs cp_async_wait_all and no block barrier)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The eight links of the hop at one output site (forward U_mu(x) in slots 0..3,
+// backward U_mu(x - mu) in slots 4..7) of 18-real FP16 links, copied once into
+// shared memory and read from there by every right-hand side of the site.
+// Slot k of thread t: x[(2k + w) * BLOCK + t] (w = 0, 1), z[k * BLOCK + t].
+template <int BLOCK>
+struct LinksF16x18Smem {
+    using R = float;
+    uint4 *x;
+    unsigned *z;
+    int outpar;  // parity of the output site: par == outpar selects the forward slots
+    __device__ __forceinline__ void stage(const LinksF16x18 &U, const SiteNbrs &n, int i) const {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int dir = k & 3;
+            const int pd = (k < 4 ? outpar : 1 - outpar) * 4 + dir;
+            const int idx = k < 4 ? i : n.bwd[dir];
+            cp_async16(x + (2 * k) * BLOCK + t, U.p + (size_t)(2 * pd) * U.stride + idx);
+            cp_async16(x + (2 * k + 1) * BLOCK + t, U.p + (size_t)(2 * pd + 1) * U.stride + idx);
+            cp_async4(z + k * BLOCK + t, U.q + (size_t)pd * U.stride + idx);
+        }
+    }
+    __device__ __forceinline__ void load(int par, int dir, int, Su3<float> &u) const {
+        const int k = (par == outpar ? 0 : 4) + dir;
+        const int t = threadIdx.x;
+        const uint4 a[2] = {x[(2 * k) * BLOCK + t], x[(2 * k + 1) * BLOCK + t]};
+        LinksF16x18::unpack(a, z[k * BLOCK + t], u);
     }
 };
 
