@@ -66,9 +66,9 @@ ITERS_PER_SOLVE = {"cg": 59, "mrhs": 59, "cg8": None}
 P4_TRAFFIC_PER_SITE_12 = 999.2e6 / 165888
 
 # DRAM traffic of the two k_hop launches of one even-odd apply (12-real FP64 links), per
-# output site, from one ncu capture at 32^4 (524,288 sites): every array is read once, so
-# it scales with the sites.  None until a capture of the current kernels is recorded.
-HOP_F64_12_TRAFFIC_PER_SITE = None
+# output site: 633.6 MB + 865.3 MB over 524,288 sites in one ncu capture at 32^4; every
+# array is read once, so it scales with the sites.
+HOP_F64_12_TRAFFIC_PER_SITE = (633.6e6 + 865.3e6) / 524288
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -199,13 +199,15 @@ def engine_phase_bytes(phase: str, vh: int, nrhs: int, prec: str, link_format: i
 
     Low-precision spinor: FP16 48 B + 4 B norm, FP32 96 B; links of the inner phases:
     all 4 V links once (FP16 18 reals, 36 B; FP32 12 reals, 48 B); y (FP32 96 B); FP64
-    spinor 192 B and FP64 links (144 or 96 B) in the reliable update."""
+    spinor 192 B and FP64 links (144 or 96 B) in the reliable update.  The reliable update
+    of M x = b (the batched solves): R1 x += y; R2 t64 = H x; R3 s = b - M x into y as
+    FP32; R4L t = H s (FP32 in, FP32 out); R5L r = M^dag s from t and y, y cleared."""
     sp = 52 if prec == "f16" else 96
     lk = 8 * (36 if prec == "f16" else 48)
     lk64 = 8 * (144 if link_format == 18 else 96)
     per = {"P1": (2 * sp, lk), "P2": (3 * sp, lk), "P3": (2 * sp, lk), "P4": (6 * sp + 2 * 96, lk),
-           "R1": (2 * 192 + 2 * 96, 0), "R2": (2 * 192, lk64), "R3": (4 * 192 + sp, lk64),
-           "R4": (2 * 192, lk64), "R4L": (2 * sp, lk), "R5": (3 * 192 + sp, lk64), "R5L": (3 * sp, lk),
+           "R1": (2 * 192 + 96, 0), "R2": (2 * 192, lk64), "R3": (3 * 192 + 96, lk64),
+           "R4": (2 * 192, lk64), "R4L": (2 * 96, lk), "R5": (3 * 192 + sp, lk64), "R5L": (3 * 96 + sp, lk),
            "P5": (3 * sp, 0)}
     pair, links = per[phase]
     return int(vh * (nrhs * pair + links))

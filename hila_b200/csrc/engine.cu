@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
 
 // ------------------------------------------------------------------ vector phases
 
-// R1: x += y; y = 0 (slots with a pending reliable update)
+// R1: x += y; y = 0 for the normal system (slots with a pending reliable update)
 // P5: p = r + beta p, or p = r on a slot's first iteration (running slots)
 template <int PHASE, int LOW>
 __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
@@ -556,7 +556,8 @@ __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
                     stc(pr.x, stride, c, i, xv);
                     y.s[c / 3][c % 3] = {0.f, 0.f};
                 }
-                ys.store(i, y);
+                // M x = b: R3 overwrites y with s and R5L clears it, so only the normal system clears here
+                if (pr.mode == ENG_MODE_NORMAL) ys.store(i, y);
             } else {
                 Spinor<float> r, p;
                 L::sp(pr.r, pr.rn, stride).load_cached(i, r);

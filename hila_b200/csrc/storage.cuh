@@ -151,12 +151,10 @@ struct SpinorF16 {
     uint4 *p;
     float *norm;
     int stride;
-    __device__ __forceinline__ void load(int i, Spinor<float> &w) const {
-        float nrm = __ldg(norm + i);
+    static __device__ __forceinline__ void unpack(const uint4 (&v)[3], float nrm, Spinor<float> &w) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            uint4 v = __ldg(p + (size_t)k * stride + i);
-            const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+            const __half2 *h = reinterpret_cast<const __half2 *>(&v[k]);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 float2 f = __half22float2(h[q]);
@@ -165,7 +163,12 @@ struct SpinorF16 {
             }
         }
     }
+    __device__ __forceinline__ void load(int i, Spinor<float> &w) const {
+        const uint4 v[3] = {__ldg(p + i), __ldg(p + (size_t)stride + i), __ldg(p + (size_t)2 * stride + i)};
+        unpack(v, __ldg(norm + i), w);
+    }
     __device__ __forceinline__ void load_cached(int i, Spinor<float> &w) const { load(i, w); }
+
     // unscaled values; the caller multiplies by *sc (the site norm)
     __device__ __forceinline__ void load_raw(int i, Spinor<float> &w, float &sc) const {
         sc = __ldg(norm + i);
