@@ -20,6 +20,9 @@ benchmark configurations; no external data):
           1..12 sources, kappa in [0.115, 0.124], accuracy 1e-10, through the
           continuous-batching server; the same request sequence is also served by the
           plain FP64 CG one source at a time (FIFO).  metric: solves/s, p50/p99 latency.
+  serve32 the mrhs workload served: 16 requests of 12 sources on the 32^4 lattice at
+          kappa = 0.124, arriving at 10 requests/s (faster than they are served),
+          against the FP64 CG serving the same stream (speedup_vs_fifo_f64_capacity).
 
 Multi-GPU runs (torchrun) are replicas: every rank solves its own copy of the
 workload; value = total solves over all ranks / max-over-ranks device time.
@@ -54,6 +57,11 @@ WORKLOADS = {
                   lattices=[(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (20, 20, 20, 20),
                             (24, 24, 24, 24), (28, 28, 28, 28), (32, 32, 32, 32)],
                   requests=200, rate=6.0, kappa_range=(0.115, 0.124), nrhs_range=(1, 12)),
+    # the headline 32^4 kappa = 0.124 workload served: requests of 12 sources each arriving faster
+    # than the GPU finishes them (saturating), against the FP64 CG serving the same stream
+    "serve32": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101,
+                    lattices=[(32, 32, 32, 32)], requests=16, rate=10.0, kappa_range=(0.124, 0.124),
+                    nrhs_range=(12, 12), pool=12),
 }
 # CG iterations of one solve of each workload (FP64 CG on M^dag M, true residual 1e-10), used to turn the
 # reference arm's per-iteration time into solves/s.  Measured by the FP64 GPU CG on exactly these seeded
@@ -467,12 +475,13 @@ def serve_stream(w, seed=11):
     rng = np.random.default_rng(seed)
     t, reqs = 0.0, []
     lo, hi = w["nrhs_range"]
+    pool = w.get("pool", SERVE_POOL)
     for n in range(w["requests"]):
         t += rng.exponential(1.0 / w["rate"])
         g = int(rng.integers(0, len(w["lattices"])))
         nrhs = int(rng.integers(lo, hi + 1))
         kappa = float(rng.uniform(*w["kappa_range"]))
-        reqs.append((t, g, kappa, [(n + k) % SERVE_POOL for k in range(nrhs)]))
+        reqs.append((t, g, kappa, [(n + k) % pool for k in range(nrhs)]))
     return reqs
 
 
@@ -490,15 +499,16 @@ def run_serve(args, dist: Dist):
     import hila_b200 as hw
     torch.cuda.set_device(dist.local_rank)
     dist.init("nccl")
-    w = WORKLOADS["serve"]
+    w = WORKLOADS[args.workload]
     ctx = hw.Context(dist.local_rank)
     reqs = serve_stream(w, seed=11 + dist.rank)
+    pool = w.get("pool", SERVE_POOL)
     lats, gauges, pools = [], [], []
     for i, dims in enumerate(w["lattices"]):
         lat = hw.Lattice(ctx, dims, True)
         lats.append(lat)
         gauges.append(hw.GaugeField(lat, hw.generate_links(dims, w["eps"], w["link_seed"] + i), args.link_format))
-        pools.append([hw.generate_spinor(dims, w["src_seed"] + 100 * i + k, hw.EVEN) for k in range(SERVE_POOL)])
+        pools.append([hw.generate_spinor(dims, w["src_seed"] + 100 * i + k, hw.EVEN) for k in range(pool)])
     srv = hw.Server(ctx, precision=args.precision, delta=args.delta)
     gids = [srv.add_gauge(G) for G in gauges]
     # warm-up: one request per lattice (graphs and tables built, memory pools grown)
@@ -570,12 +580,13 @@ def run_serve(args, dist: Dist):
     fifo_rate = solves / t_free  # wall rate of the FIFO schedule of this stream
     fifo_capacity = solves / busy
     out = {
-        "metric": "served CG solves/s at 1e-10 residual (Poisson stream, 8 lattices)", "value": round(value, 4),
+        "metric": "served CG solves/s at 1e-10 residual (Poisson stream, %d lattices)" % len(lats),
+        "value": round(value, 4),
         "unit": "solves/s", "n_gpus": dist.world, "steps": len(reqs), "warmup": len(lats),
         "ms_per_step": round(1e3 * t_wall / len(reqs), 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"f32": "f32+f64", "f16": "f16+f64"}[args.precision],
         "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources, Poisson arrivals",
-        "config": {"workload": "serve", "lattices": ["x".join(map(str, d)) for d in w["lattices"]],
+        "config": {"workload": args.workload, "lattices": ["x".join(map(str, d)) for d in w["lattices"]],
                    "requests": len(reqs), "rate_per_s": w["rate"], "nrhs_range": w["nrhs_range"],
                    "kappa_range": w["kappa_range"], "tol": w["tol"], "link_format": args.link_format,
                    "precision": args.precision, "delta": args.delta, "parallelism": f"replicas{dist.world}"},
@@ -587,6 +598,7 @@ def run_serve(args, dist: Dist):
         "submit_lag_ms_max": round(1e3 * max(ts - (t0 + r[0]) for ts, r in zip(t_sub, reqs)), 3),
         "all_converged": ok, "max_true_residual": max(r.true_residual for r in results),
         "spot_check_residual": chk, "solves": solves, "wall_s": round(t_wall, 3),
+        "speedup_vs_fifo_f64_capacity": round(value / fifo_capacity, 3),
         "fifo_f64": {"solves_per_s": round(fifo_rate, 3), "capacity_solves_per_s": round(fifo_capacity, 3),
                      "latency_ms_p50": pct(lat64, 0.5), "latency_ms_p99": pct(lat64, 0.99),
                      "all_converged": ok64},
@@ -612,7 +624,7 @@ def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return
     w = WORKLOADS[args.workload]
-    if args.workload == "serve":
+    if args.workload.startswith("serve"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; its FP64 CG "
                           "is timed on the cg and mrhs workloads"}), flush=True)
         return
@@ -652,7 +664,7 @@ def main():
     ap.add_argument("--workload", default="mrhs", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["f64", "f32", "f16"],
-                    help="default: f16 for mrhs/serve, f64 otherwise")
+                    help="default: f16 for mrhs/serve/serve32, f64 otherwise")
     ap.add_argument("--link-format", type=int, default=12, choices=[18, 12])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="CG iterations from a host loop (for launch lists)")
@@ -664,13 +676,13 @@ def main():
     ap.add_argument("--rate", type=float, default=None, help="serve: Poisson arrival rate (requests/s)")
     args = ap.parse_args()
     if args.precision is None:
-        args.precision = "f16" if args.workload in ("mrhs", "serve") else "f64"
+        args.precision = "f16" if args.workload in ("mrhs", "serve", "serve32") else "f64"
     if args.delta is None:
         args.delta = 1e-5 if args.precision == "f32" else 0.005
-    if args.requests:
-        WORKLOADS["serve"]["requests"] = args.requests
-    if args.rate:
-        WORKLOADS["serve"]["rate"] = args.rate
+    if args.requests and args.workload.startswith("serve"):
+        WORKLOADS[args.workload]["requests"] = args.requests
+    if args.rate and args.workload.startswith("serve"):
+        WORKLOADS[args.workload]["rate"] = args.rate
     if args.lattice:
         WORKLOADS[args.workload]["dims"] = tuple(int(v) for v in args.lattice.split("x"))
     if args.nrhs:
@@ -682,7 +694,7 @@ def main():
     dist = Dist()
     if args.impl == "reference":
         run_reference(args, dist)
-    elif args.workload == "serve":
+    elif args.workload.startswith("serve"):
         run_serve(args, dist)
     else:
         run_ours(args, dist)

@@ -230,7 +230,9 @@ void launch_variant(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin
 
 // Launch shapes the autotuner chooses from (HopVariant in kernels.h):
 //   0: 128 threads, registers unconstrained   1: 128 threads, <= 128 registers (4 blocks/SM)
-//   2: 256 threads, <= 128 registers          3: 128 threads, <= 102 registers (5 blocks/SM)
+//   2: 256 threads, <= 128 registers
+// (128 threads at <= 102 registers spills about 600 bytes per thread and measured 0.63 of
+// HBM peak against 0.80-0.83 for these.)
 template <class Lk, class Epi>
 void launch_shape(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin, const Epi &epi, RedBuf rb,
                   cudaStream_t s) {
@@ -240,9 +242,6 @@ void launch_shape(const Geom &g, const Lk &L, int par, int sign, SpinorF64 sin, 
         break;
     case 2:
         launch_variant<256, 2>(g, L, par, sign, sin, epi, rb, s);
-        break;
-    case 3:
-        launch_variant<128, 5>(g, L, par, sign, sin, epi, rb, s);
         break;
     default:
         launch_variant<128, 1>(g, L, par, sign, sin, epi, rb, s);

@@ -86,6 +86,31 @@ __device__ __forceinline__ void stc(double2 *p, int stride, int c, int i, Cx<dou
     p[(size_t)c * stride + i] = make_double2(v.re, v.im);
 }
 
+static_assert(kEngMaxRhs <= 32, "one warp lane per slot of a lattice");
+
+// Active slots of every lattice for one phase launch, built once per block: slot
+// states change only in the finishers, and a lattice's finisher runs after all of
+// its work items, so the table stays valid for every item the block still meets.
+struct ActiveTable {
+    int slot[kEngMaxLat][kEngMaxRhs];  // slot[l][a]: the a-th active slot of lattice l
+    int n[kEngMaxLat];
+};
+
+template <int PHASE>
+__device__ __forceinline__ void build_active(const EngPtrs &P, ActiveTable &A) {
+    const EngTables *T = P.T;
+    for (int l = threadIdx.x; l < T->nlat; l += blockDim.x) {
+        const EngLattice &La = T->lat[l];
+        int na = 0;
+        for (int q = 0; q < La.nprob; q++) {
+            const int j = La.prob[q];
+            if (active<PHASE>(P.S[j])) A.slot[l][na++] = j;
+        }
+        A.n[l] = na;
+    }
+    __syncthreads();
+}
+
 // ------------------------------------------------------------------ epilogues
 
 // Low-precision phases P1..P4.  acc = (H in)(i) in FP32.
@@ -364,13 +389,18 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
         const int lt = tile - La.tile0;
         const int i = lt * kEngTile + threadIdx.x;
         const bool valid = i < g.Vh;
-        if (threadIdx.x == 0) {
-            int na = 0;
-            for (int q = 0; q < La.nprob; q++) {
-                const int j = La.prob[q];
-                if (active<PHASE>(P.S[j])) s_act[na++] = j;
+        if (threadIdx.x < 32) {
+            // the lattice's active slots in list order: one lane per slot, one ballot
+            const int q = threadIdx.x;
+            int j = 0;
+            bool on = false;
+            if (q < La.nprob) {
+                j = La.prob[q];
+                on = active<PHASE>(P.S[j]);
             }
-            s_na = na;
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (on) s_act[__popc(m & ((1u << q) - 1u))] = j;
+            if (q == 0) s_na = __popc(m);
         }
         __syncthreads();
         const int na = s_na;
@@ -472,26 +502,20 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
     using Lk = typename std::conditional<PLANES == 9, LinksF64x18, LinksF64x12>::type;
     __shared__ double smem[kEngTile / 32];
     __shared__ bool last;
+    __shared__ ActiveTable act;
     if (*(volatile int *)(P.ctl + 2) == 0) return;  // no reliable update pending
     const EngTables *T = P.T;
     const int nitems = T->ntiles * kEngMaxRhs;
     const int max_tiles = T->max_tiles;
+    build_active<PHASE>(P, act);
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int tile = item / kEngMaxRhs, a = item % kEngMaxRhs;
         const int l = find_lattice(T, tile);
         const EngLattice &La = T->lat[l];
-        if (La.l64_planes != PLANES || a >= La.nprob) continue;
-        // the a-th slot with a pending update (states change only in the finisher,
-        // which runs after every item of the lattice has arrived)
-        int j = -1, na = 0;
-        for (int q = 0; q < La.nprob; q++) {
-            const int jq = La.prob[q];
-            if (active<PHASE>(P.S[jq])) {
-                if (na == a) j = jq;
-                na++;
-            }
-        }
-        if (j < 0) continue;
+        const int na = act.n[l];
+        // the a-th slot with a pending update
+        if (La.l64_planes != PLANES || a >= na) continue;
+        const int j = act.slot[l][a];
         const Geom g = La.g;
         const int stride = La.stride;
         const int lt = tile - La.tile0;

@@ -11,7 +11,7 @@ namespace hw {
 
 constexpr int kHopBlock = 128;
 constexpr int kHopMinBlock = 128;  // smallest block of any hop launch shape (sizes reduction buffers)
-constexpr int kHopVariants = 4;
+constexpr int kHopVariants = 3;
 
 // Device-resident scalars of one FP64 conjugate-gradient solve
 // (conjugate_gradient.h:55-57 keeps the same quantities on the host).
