@@ -80,6 +80,7 @@ HOP_F64_12_TRAFFIC_PER_SITE = (633.6e6 + 865.3e6) / 524288
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e, nominal; reported beside the measured peak
 
 
 def hbm_peak():
@@ -196,8 +197,25 @@ def cpu_sample(workload: str, seconds_budget: float = 20.0):
     t0 = time.perf_counter()
     it, _ = R.cg(U, w["kappa"], b, x, 1e-300, n_it)
     t_cg = time.perf_counter() - t0
+    # context: one apply on one thread, and the oracle's fused operator (one pass over the
+    # output sites, no temporaries) on all cores and on one thread
+    applies = {"reference_structured": {str(cores): t_apply}, "fused": {}}
+    t0 = time.perf_counter()
+    o.eo_apply(dims, U, w["kappa"], b, 1)
+    applies["fused"][str(cores)] = time.perf_counter() - t0
+    o.set_num_threads(1)
+    try:
+        t0 = time.perf_counter()
+        R.eo_apply(U, w["kappa"], b, out, 1)
+        applies["reference_structured"]["1"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        o.eo_apply(dims, U, w["kappa"], b, 1)
+        applies["fused"]["1"] = time.perf_counter() - t0
+    finally:
+        o.set_num_threads(cores)
     R.close()
-    return dict(t_iter=t_cg / max(it, 1), iters=it, t_apply=t_apply, cores=cores, dims=dims)
+    return dict(t_iter=t_cg / max(it, 1), iters=it, t_apply=t_apply, cores=cores, dims=dims,
+                apply_seconds={k: {n: round(t, 4) for n, t in v.items()} for k, v in applies.items()})
 
 
 # ------------------------------------------------------------------ our arm
@@ -419,6 +437,7 @@ def run_ours(args, dist: Dist):
                        "source": "ncu capture at 32^4 (mean of the apply's two launches) scaled by sites"}
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "frac_of_nominal_8000": round(achieved / NOMINAL_HBM_GBS, 4),
                 "traffic": hop_traffic, "kernel": "k_hop (FP64, %d-real links)" % args.link_format,
                 "algorithmic_bytes_per_launch": apply_bytes / 2}
     if args.workload == "mrhs":
@@ -453,11 +472,13 @@ def run_ours(args, dist: Dist):
                                "sample": f"{cs['iters']} CG iterations of the reference-structured oracle at "
                                          f"{'x'.join(map(str, cs['dims']))} on {cs['cores']} threads "
                                          f"({cs['t_iter']:.3f} s/iteration), scaled by the {iters} iterations "
-                                         f"of one solve"}
+                                         f"of one solve",
+                               "apply_seconds_by_threads": cs["apply_seconds"]}
     elif dist.rank == 0 and dist.world == 1 and args.workload == "dslash" and not args.no_cpu_baseline:
         cs = cpu_sample("cg", seconds_budget=5.0)
         out["cpu_baseline"] = {"value": apply_bytes / cs["t_apply"] / 1e9, "unit": "GB/s", "cores": cs["cores"],
-                               "kind": "port", "sample": "one reference-structured even-odd apply at 32^4"}
+                               "kind": "port", "sample": "one reference-structured even-odd apply at 32^4",
+                               "apply_seconds_by_threads": cs["apply_seconds"]}
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
     for f in (fb, fx):
@@ -635,13 +656,35 @@ def run_reference(args, dist: Dist):
         value = (2 * (8 * 144 + 384) + 192) * (V // 2) / t / 1e9
         unit, cs, sample = "GB/s", samples[0], "one reference-structured even-odd apply per step"
         ms_per_step = t * 1e3
+    elif ITERS_PER_SOLVE.get(args.workload) is None:
+        # small enough for whole solves: the reference-structured CG on M^dag M to its own
+        # stopping rule (|r|^2 < acc^2 |b|^2, conjugate_gradient.h:63,91), one solve per step
+        from oracle import oracle as o
+        o.build()
+        dims = w["dims"]
+        U = o.gen_links(dims, w["eps"], w["link_seed"])
+        b = o.gen_spinor(dims, w["src_seed"], o.EVEN)
+        R = o.RefStructured(dims)
+        times, its = [], []
+        for k in range(args.warmup + args.steps):
+            x = np.zeros_like(b)
+            t0 = time.perf_counter()
+            it, _ = R.cg(U, w["kappa"], b, x, w["tol"], 10000)
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+                its.append(it)
+        R.close()
+        t_solve = statistics.mean(times)
+        value, unit = 1.0 / t_solve, "solves/s"
+        cs = {"cores": o.num_threads()}
+        sample = (f"whole solves of the reference-structured CG at {'x'.join(map(str, dims))} "
+                  f"({its[0]} iterations to its stopping rule, {t_solve:.4f} s each)")
+        ms_per_step = t_solve * 1e3
     else:
         iters = ITERS_PER_SOLVE.get(args.workload)
         samples = [cpu_sample(args.workload, seconds_budget=15.0) for _ in range(args.warmup + args.steps)]
         samples = samples[args.warmup:]
         t_iter = statistics.mean(s["t_iter"] for s in samples)
-        if iters is None:
-            iters = 1
         value = 1.0 / (t_iter * iters)
         unit, cs = "solves/s", samples[0]
         sample = (f"{cs['iters']} CG iterations per step of the reference-structured oracle, scaled by the "
