@@ -1,5 +1,5 @@
 """The full-size benchmark configurations of the mixed-precision and batched solves,
-judged by size-independent properties: every solve's true residual |b - M x| / |b|
+checked by size-independent properties: every solve's true residual |b - M x| / |b|
 recomputed by the CPU oracle in FP64 (<= 1e-10), agreement with the plain FP64 CG,
 and bitwise batch invariance (a solve alone and in the mix)."""
 import time

@@ -1,6 +1,6 @@
 """GPU tests of the mixed-precision solves and of the batched engine.
 
-Every solve is judged by its true residual |b - M x| / |b| recomputed by the
+Every solve is checked by its true residual |b - M x| / |b| recomputed by the
 CPU oracle in FP64: <= 1e-10.  Batched solves must give bitwise the same
 solution alone and inside a batch.
 """
