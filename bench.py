@@ -227,7 +227,8 @@ def engine_phase_bytes(phase: str, vh: int, nrhs: int, prec: str, link_format: i
     all 4 V links once (FP16 18 reals, 36 B; FP32 12 reals, 48 B); y (FP32 96 B); FP64
     spinor 192 B and FP64 links (144 or 96 B) in the reliable update.  The reliable update
     of M x = b (the batched solves): R1 x += y; R2 t64 = H x; R3 s = b - M x into y as
-    FP32; R4L t = H s (FP32 in, FP32 out); R5L r = M^dag s from t and y, y cleared."""
+    FP32; R4L t = H s (FP32 in, FP32 out); R5L r = M^dag s from t and y, y cleared.  A
+    solve's first update from x = 0 skips R2 and R3's hop, so those launches move less."""
     sp = 52 if prec == "f16" else 96
     lk = 8 * (36 if prec == "f16" else 48)
     lk64 = 8 * (144 if link_format == 18 else 96)

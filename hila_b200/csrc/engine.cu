@@ -72,6 +72,8 @@ __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
 // which run after every tile of the lattice is done, so all blocks agree.
 template <int PHASE>
 __device__ __forceinline__ bool active(const EngState &s) {
+    // the first update of a solve from x = 0: H x is zero, R2 has nothing to do
+    if (PHASE == PH_R2) return s.ru != 0 && !(s.init && !s.xnz);
     if (PHASE == PH_R4 || PHASE == PH_R5) return s.ru != 0 && s.mode == ENG_MODE_NORMAL;
     if (PHASE == PH_R4L || PHASE == PH_R5L) return s.ru != 0 && s.mode == ENG_MODE_SOLVE;
     if (eng_ru_phase(PHASE)) return s.ru != 0;
@@ -530,10 +532,15 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
             Spinor<double> acc;
 #pragma unroll
             for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = {0.0, 0.0};
-            hop_dir_lean<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir_lean<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir_lean<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
-            hop_dir_lean<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            // R3 of a first update from x = 0: R2 was skipped and H t64 = 0, so s = b with
+            // the same bits the hop of zeros would give (b - (+-0) = b)
+            const bool zero_in = PHASE == PH_R3 && P.S[j].init && !P.S[j].xnz;
+            if (!zero_in) {
+                hop_dir_lean<0, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                hop_dir_lean<1, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                hop_dir_lean<2, SIGN>(nb, OUTPAR, i, sin, U, acc);
+                hop_dir_lean<3, SIGN>(nb, OUTPAR, i, sin, U, acc);
+            }
             epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
         }
         if constexpr (NRED > 0) {
@@ -573,12 +580,22 @@ __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
                 Spinor<float> y;
                 ys.load_cached(i, y);
 #pragma unroll
+                bool nz = false;
+#pragma unroll
                 for (int c = 0; c < 12; c++) {
                     Cx<double> xv = ldc(pr.x, stride, c, i);
+                    nz |= xv.re != 0.0 || xv.im != 0.0;
                     xv.re += (double)y.s[c / 3][c % 3].re;
                     xv.im += (double)y.s[c / 3][c % 3].im;
                     stc(pr.x, stride, c, i, xv);
                     y.s[c / 3][c % 3] = {0.f, 0.f};
+                }
+                // first update: record whether the initial x is nonzero anywhere (one atomic
+                // per warp at most; the flag is read by R2 and R3 after this launch)
+                if (s.init) {
+                    const unsigned am = __activemask();
+                    if (__any_sync(am, nz) && (threadIdx.x & 31) == __ffs(am) - 1 && !*(volatile int *)&P.S[j].xnz)
+                        atomicOr(&P.S[j].xnz, 1);
                 }
                 // M x = b: R3 overwrites y with s and R5L clears it, so only the normal system clears here
                 if (pr.mode == ENG_MODE_NORMAL) ys.store(i, y);

@@ -90,7 +90,7 @@ struct EngState {
     int init;        // 1: first reliable update (r from x), p = r afterwards
     int n_ru;
     int mode;        // EngMode of the slot (copy of its problem's, read by the phase selection)
-    int pad;
+    int xnz;         // 1: the initial x has a nonzero component (set by R1 of the first update)
 };
 
 struct EngTables {

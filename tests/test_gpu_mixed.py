@@ -53,6 +53,45 @@ def test_mixed_normal_equations(hw, ctx, oracle, precision):
     assert oracle.true_residual_normal(dims, U, 0.12, src, fout.download()) <= TOL
 
 
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_mixed_initial_guess(hw, ctx, oracle, precision):
+    """The solve starts from the x it is given (CG<Op>::apply starts from `out`).  A guess
+    near the solution saves iterations; a guess that is nonzero on a single component must
+    still be used (the first reliable update skips its FP64 hops only when x is zero
+    everywhere); and a batch mixing zero and nonzero guesses gives bitwise the same
+    solutions as each request alone."""
+    dims, kappa = (8, 8, 8, 8), 0.12
+    U, lat, G = make(hw, ctx, oracle, dims, 61)
+    b = oracle.gen_spinor(dims, 62, oracle.EVEN)
+    D = hw.Dirac_Wilson_evenodd(kappa, G)
+    fb = hw.Field(lat, b)
+    fx0 = hw.Field(lat)
+    r0 = D.solve(fb, fx0, accuracy=TOL, precision=precision)
+    assert r0.converged
+    near = fx0.download() + 1e-4 * oracle.gen_spinor(dims, 63, oracle.EVEN)
+    fx = hw.Field(lat, near)
+    r = D.solve(fb, fx, accuracy=TOL, precision=precision)
+    assert r.converged and r.iterations < r0.iterations, (r.iterations, r0.iterations)
+    assert oracle.true_residual(dims, U, kappa, b, fx.download()) <= TOL
+    even = np.flatnonzero(oracle.parity_mask(dims) == 0)
+    spike = np.zeros_like(b)
+    spike[even[len(even) // 2], 2, 1, 0] = 3.0
+    fs = hw.Field(lat, spike)
+    rs = D.solve(fb, fs, accuracy=TOL, precision=precision)
+    assert rs.converged
+    assert oracle.true_residual(dims, U, kappa, b, fs.download()) <= TOL
+    # batched: a zero guess and the single-component guess together, then each alone
+    fz, fsp = hw.Field(lat), hw.Field(lat, spike)
+    both = hw.batch_solve(ctx, [(D, fb, fz, TOL), (D, fb, fsp, TOL)], precision=precision)
+    assert all(q.converged for q in both)
+    for guess, fout, res in ((None, fz, both[0]), (spike, fsp, both[1])):
+        alone = hw.Field(lat) if guess is None else hw.Field(lat, guess)
+        [ra] = hw.batch_solve(ctx, [(D, fb, alone, TOL)], precision=precision)
+        assert ra.iterations == res.iterations
+        assert np.array_equal(alone.download(), fout.download())
+        assert oracle.true_residual(dims, U, kappa, b, fout.download()) <= TOL
+
+
 def test_mixed_edge_cases(hw, ctx, oracle):
     dims = (4, 4, 4, 4)
     U, lat, G = make(hw, ctx, oracle, dims, 31)
