@@ -9,6 +9,8 @@
 // multiplies by the link and expands in registers, and the epilogue fuses
 // whatever the caller does next (scaling, the diagonal term of the even-odd
 // operator, the CG axpy updates and their dot products).
+#include <mutex>
+
 #include "kernels.h"
 #include "reduce.cuh"
 #include "storage.cuh"
@@ -202,18 +204,24 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_hop(Geom g, Lk U, int par, Spin
     if constexpr (Epi::NRED > 0) grid_reduce<Epi::NRED, BLOCK>(v, red.partials, red.ticket, epi);
 }
 
-// shared memory of the staged epilogue operands; near the 48 KB default the kernel
-// is opted in once (per instantiation)
+// shared memory of the staged epilogue operands.  Near the 48 KB default the kernel is
+// opted in to more, once per instantiation and device (the attribute belongs to the
+// device that is current when it is set; contexts on several GPUs share one process).
+// If the opt-in fails the launch itself reports the error.
 template <int SIGN, int BLOCK, int MINB, class Lk, class Epi>
 size_t hop_smem() {
     constexpr size_t bytes = (size_t)Epi::NPRE * 12 * BLOCK * sizeof(double2);
     if constexpr (bytes > 32 * 1024) {
-        static const bool once = [] {
-            cudaFuncSetAttribute(k_hop<SIGN, BLOCK, MINB, Lk, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)bytes);
-            return true;
-        }();
-        (void)once;
+        static std::mutex mu;
+        static unsigned long long done = 0;  // bit d: set on device d
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!((done >> dev) & 1ull) &&
+                cudaFuncSetAttribute(k_hop<SIGN, BLOCK, MINB, Lk, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes) == cudaSuccess)
+                done |= 1ull << dev;
+        }
     }
     return bytes;
 }
