@@ -69,3 +69,43 @@ def test_generators_match_oracle(hw, oracle):
         s1 = hw.generate_spinor(dims, 5, par)
         s2 = oracle.gen_spinor(dims, 5, par)
         assert np.array_equal(s1, s2)
+
+
+C_CONSUMER = r"""
+#include "hila_b200.h"
+#include <stdio.h>
+#include <stdlib.h>
+int main(void) {
+    int dims[4] = {4, 4, 4, 2};
+    double *U = malloc(sizeof(double) * 4 * 128 * 18);
+    int rc = hw_generate_links(dims, 0.3, 7, U);
+    printf("%d %d %.17g %.17g\n", hw_api_version(), rc, U[0], U[4 * 128 * 18 - 1]);
+    free(U);
+    return rc;
+}
+"""
+
+
+def test_header_is_c99_and_links_from_c(hw, lib, tmp_path):
+    """A plain C program (no C++) includes the header under -std=c99 -pedantic, links the
+    library and calls it: what a cgo or C caller sees."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    src = tmp_path / "consumer.c"
+    src.write_text(C_CONSUMER)
+    exe = tmp_path / "consumer"
+    libdir = os.path.dirname(hw.LIB_PATH)
+    libname = os.path.basename(hw.LIB_PATH)[3:-3]
+    cc = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                         os.path.join(ROOT, "include"), str(src), "-L", libdir, "-l" + libname,
+                         "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stderr
+    version, rc, first, last = run.stdout.split()
+    assert int(rc) == 0 and int(version) >= 1
+    U = hw.generate_links((4, 4, 4, 2), 0.3, 7)
+    assert float(first) == U.reshape(-1)[0] and float(last) == U.reshape(-1)[-1]
