@@ -36,7 +36,6 @@ __device__ __forceinline__ SpinorF64 staged(double2 *stage, int block, int k) {
 struct EpiScale {
     static constexpr int NRED = 0;
     static constexpr int NPRE = 0;
-    __device__ SpinorF64 pre(int) const { return out; }
     SpinorF64 out;
     double a;
     const CgState *st;
@@ -46,7 +45,6 @@ struct EpiScale {
         for (int c = 0; c < 12; c++) acc.s[c / 3][c % 3] = a * acc.s[c / 3][c % 3];
         out.store(i, acc);
     }
-    __device__ void operator()(const double *) {}
 };
 
 // Component c (0..11) of a half-lattice FP64 field at site i

@@ -457,9 +457,8 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
                     hop_dir_pair<3, SIGN>(nb, OUTPAR, i, in[0], in[1], U, a2);
 #pragma unroll
                     for (int c = 0; c < 12; c++) {
-                        const Cx2 v = a2.s[c / 3][c % 3];
-                        acc[0].s[c / 3][c % 3] = {v.re.x, v.im.x};
-                        acc[NR - 1].s[c / 3][c % 3] = {v.re.y, v.im.y};
+                        acc[0].s[c / 3][c % 3] = {a2.s[c / 3][c % 3].re.x, a2.s[c / 3][c % 3].im.x};
+                        acc[NR - 1].s[c / 3][c % 3] = {a2.s[c / 3][c % 3].re.y, a2.s[c / 3][c % 3].im.y};
                     }
                 } else {
                     hop_dir_multi<0, SIGN>(nb, OUTPAR, i, in, cnt, U, acc);
@@ -579,7 +578,6 @@ __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
                 SpinorF32 ys{pr.y, stride};
                 Spinor<float> y;
                 ys.load_cached(i, y);
-#pragma unroll
                 bool nz = false;
 #pragma unroll
                 for (int c = 0; c < 12; c++) {

@@ -235,7 +235,6 @@ int admit_waiting(hw_server *S) {
         q->bytes = need;
         S->bytes_in_use += need;
         q->t_admit = Clock::now();
-        hw_context *ctx = S->ctx;
         const int stride = E.lattice(l).stride;
         for (int k = 0; k < q->nrhs; k++) {
             int slot;
