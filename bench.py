@@ -15,7 +15,7 @@ benchmark configurations; no external data):
           updates), next to the plain FP64 CG on the same workload in the same run.
           metric: CG solves/s (mixed), with fp64_solves_per_s and the speed-up.
   cg8     8^4, kappa = 0.12, plain FP64 CG (the CPU-runnable configuration).
-  serve   Poisson stream of solve requests (default 200 at 6 requests/s; --requests,
+  serve   Poisson stream of solve requests (default 2000 at 20 requests/s; --requests,
           --rate) over 8 device-resident gauge fields 8^4 .. 32^4, each request with
           1..12 sources, kappa in [0.115, 0.124], accuracy 1e-10, through the
           continuous-batching server; the same request sequence is also served by the
@@ -56,7 +56,7 @@ WORKLOADS = {
     "serve": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101,
                   lattices=[(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32), (20, 20, 20, 20),
                             (24, 24, 24, 24), (28, 28, 28, 28), (32, 32, 32, 32)],
-                  requests=200, rate=6.0, kappa_range=(0.115, 0.124), nrhs_range=(1, 12)),
+                  requests=2000, rate=20.0, kappa_range=(0.115, 0.124), nrhs_range=(1, 12)),
     # the headline 32^4 kappa = 0.124 workload served: requests of 12 sources each arriving faster
     # than the GPU finishes them (saturating), against the FP64 CG serving the same stream
     "serve32": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101,
@@ -220,24 +220,71 @@ def cpu_sample(workload: str, seconds_budget: float = 20.0):
 
 # ------------------------------------------------------------------ our arm
 
-def engine_phase_bytes(phase: str, vh: int, nrhs: int, prec: str, link_format: int) -> int:
-    """Algorithmic bytes of one engine phase launch: every array read or written once.
+def engine_unit_bytes(phase: str, prec: str, link_format: int) -> tuple:
+    """Algorithmic bytes of one work unit of an engine phase (every array read or written once).
 
-    Low-precision spinor: FP16 48 B + 4 B norm, FP32 96 B; links of the inner phases:
-    all 4 V links once (FP16 18 reals, 36 B; FP32 12 reals, 48 B); y (FP32 96 B); FP64
-    spinor 192 B and FP64 links (144 or 96 B) in the reliable update.  The reliable update
-    of M x = b (the batched solves): R1 x += y; R2 t64 = H x; R3 s = b - M x into y as
-    FP32; R4L t = H s (FP32 in, FP32 out); R5L r = M^dag s from t and y, y cleared.  A
-    solve's first update from x = 0 skips R2 and R3's hop, so those launches move less."""
+    Returns (main, alternate, link site, normal-system R3) bytes for the four counters of
+    the engine profile (hw_engine_profile.work).  Low-precision spinor `sp`: FP16 48 B + 4 B
+    norm, FP32 96 B; y and the FP32 s / t of the reliable update 96 B; FP64 spinor 192 B.
+    Links: all 8 links of a site once per launch (inner phases FP16 18 reals = 36 B or FP32
+    12 reals = 48 B; FP64 144 or 96 B in R2..R5).  Arrays per slot and site:
+      P1  p (neighbours) read, t written                           2 sp
+      P2  t (neighbours), p read; Dp written                       3 sp
+      P3  Dp (neighbours) read, t written                          2 sp
+      P4  t (neighbours), Dp, r, p read; r written; y read+written 5 sp + 2 x 96
+      R1  x read+written, y read (alternate: y also cleared)       2 x 192 + 96 (+ 96)
+      R2  x (neighbours) read, t64 written                         2 x 192
+      R3  t64 (neighbours), x, b read; s written as FP32 in y      3 x 192 + 96
+          alternate (x = 0 first update, no hop): x, b read, y     2 x 192 + 96
+          normal system: t64, x read, s written in FP64            3 x 192
+      R4  s (neighbours) read, t64 written                         2 x 192
+      R4L y (= s, neighbours) read, t written (FP32)               2 x 96
+      R5  t64 (neighbours), s, b read; r written                   3 x 192 + sp
+      R5L t (neighbours), y read; y cleared; r written             3 x 96 + sp
+      P5  r, p read; p written (alternate, first iteration: p = r) 3 sp (2 sp)"""
     sp = 52 if prec == "f16" else 96
     lk = 8 * (36 if prec == "f16" else 48)
     lk64 = 8 * (144 if link_format == 18 else 96)
-    per = {"P1": (2 * sp, lk), "P2": (3 * sp, lk), "P3": (2 * sp, lk), "P4": (6 * sp + 2 * 96, lk),
-           "R1": (2 * 192 + 96, 0), "R2": (2 * 192, lk64), "R3": (3 * 192 + 96, lk64),
-           "R4": (2 * 192, lk64), "R4L": (2 * 96, lk), "R5": (3 * 192 + sp, lk64), "R5L": (3 * 96 + sp, lk),
-           "P5": (3 * sp, 0)}
-    pair, links = per[phase]
-    return int(vh * (nrhs * pair + links))
+    table = {"P1": (2 * sp, 0, lk, 0), "P2": (3 * sp, 0, lk, 0), "P3": (2 * sp, 0, lk, 0),
+             "P4": (5 * sp + 2 * 96, 0, lk, 0), "R1": (2 * 192 + 96, 2 * 192 + 2 * 96, 0, 0),
+             "R2": (2 * 192, 0, lk64, 0), "R3": (3 * 192 + 96, 2 * 192 + 96, lk64, 3 * 192),
+             "R4": (2 * 192, 0, lk64, 0), "R4L": (2 * 96, 0, lk, 0), "R5": (3 * 192 + sp, 0, lk64, 0),
+             "R5L": (3 * 96 + sp, 0, lk, 0), "P5": (3 * sp, 2 * sp, 0, 0)}
+    return table[phase]
+
+
+def engine_phase_bytes(phase: str, work, prec: str, link_format: int) -> int:
+    """Algorithmic bytes of the work units `work` (the profile's four counters) of a phase."""
+    unit = engine_unit_bytes(phase, prec, link_format)
+    return int(sum(u * w for u, w in zip(unit, work)))
+
+
+def phase_table(prof: dict, prec: str, link_format: int, peak: float) -> dict:
+    """Per-phase launches, time and algorithmic bytes of the launches that did work."""
+    out = {}
+    for k, (n, ms, work) in prof.items():
+        if not n:
+            out[k] = {"launches": 0, "ms_per_launch": None, "bytes_per_launch": None, "gbs": None, "frac": None}
+            continue
+        byt = engine_phase_bytes(k, work, prec, link_format) / n
+        gbs = byt / (ms / n * 1e-3) / 1e9 if ms > 0 else None
+        out[k] = {"launches": n, "ms_per_launch": round(ms / n, 4), "bytes_per_launch": int(byt),
+                  "gbs": round(gbs, 1) if gbs else None, "frac": round(gbs / peak, 4) if gbs else None,
+                  "work_units": list(work)}
+    return out
+
+
+def workload_config(args, w, world: int) -> dict:
+    """The `config` of a bench line; both arms print the same one for the same workload."""
+    dims = w["dims"]
+    V = int(np.prod(dims))
+    link_bytes = 144 if args.link_format == 18 else 96
+    cfg = {"workload": args.workload, "lattice": "x".join(map(str, dims)), "kappa": w["kappa"], "eps": w["eps"],
+           "tol": w["tol"], "link_format": args.link_format, "parallelism": f"replicas{world}",
+           "l2": "inputs larger than L2 (links %d MB)" % (4 * V * link_bytes // 2**20)}
+    if "nrhs" in w:
+        cfg["nrhs"] = w["nrhs"]
+    return cfg
 
 
 def run_ours(args, dist: Dist):
@@ -379,10 +426,17 @@ def run_ours(args, dist: Dist):
         batch_once()
         prof = ctx.engine_profile_get(prec)
         ctx.engine_profile(False)
-        result["phases"] = {k: {"launches": n, "ms_per_launch": round(ms / n, 4) if n else None,
-                                "bytes_per_launch": engine_phase_bytes(k, V // 2, nrhs, prec, args.link_format)}
-                            for k, (n, ms) in prof.items()}
+        result["phases"] = phase_table(prof, prec, args.link_format, peak)
         engine_roof = result["phases"]["P4"]
+        if not args.no_served and dist.world == 1:
+            # the same 32^4 workload through the continuous-batching server (serve32: 16 requests of
+            # 12 sources arriving faster than they are served), against the plain FP64 CG serving
+            # the same stream
+            m = serve_measure(ctx, WORKLOADS["serve32"], args)
+            result["served_speedup_vs_fp64"] = m["speedup_vs_fifo_f64_capacity"]
+            result["served"] = {k: m[k] for k in ("value", "requests", "solves", "latency_ms_p50", "latency_ms_p99",
+                                                  "all_converged", "max_true_residual", "fifo_f64")}
+            result["served"]["workload"] = "serve32"
         for f in fbs + fxs:
             f.close()
     else:
@@ -458,10 +512,7 @@ def run_ours(args, dist: Dist):
         "metric": METRIC, "value": round(value, 4), "unit": unit, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": dtype, "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources",
-        "config": {"workload": args.workload, "lattice": "x".join(map(str, dims)), "kappa": w["kappa"],
-                   "eps": w["eps"], "tol": w["tol"], "link_format": args.link_format,
-                   "parallelism": f"replicas{dist.world}",
-                   "l2": "inputs larger than L2 (links %d MB)" % (4 * V * link_bytes // 2**20)},
+        "config": workload_config(args, w, dist.world),
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "impl": "ours",
         **result,
     }
@@ -515,15 +566,13 @@ def pct(v, q):
     return v[min(len(v) - 1, int(q * len(v)))] if v else None
 
 
-def run_serve(args, dist: Dist):
-    """Poisson request stream through the server, and the same stream through the FP64 CG (FIFO)."""
+def serve_measure(ctx, w, args, rank: int = 0) -> dict:
+    """Serve the Poisson request stream of workload `w` through the continuous-batching server,
+    then the same stream through the plain FP64 CG (FIFO, one source at a time).  Returns the
+    measured figures; the clocks are sampled while the server runs."""
     import torch
     import hila_b200 as hw
-    torch.cuda.set_device(dist.local_rank)
-    dist.init("nccl")
-    w = WORKLOADS[args.workload]
-    ctx = hw.Context(dist.local_rank)
-    reqs = serve_stream(w, seed=11 + dist.rank)
+    reqs = serve_stream(w, seed=11 + rank)
     pool = w.get("pool", SERVE_POOL)
     lats, gauges, pools = [], [], []
     for i, dims in enumerate(w["lattices"]):
@@ -539,9 +588,8 @@ def run_serve(args, dist: Dist):
         srv.wait(rid, 1, lats[g].volume, copy=False)
     out_pool = [[np.zeros((lat.volume, 4, 3, 2)) for _ in range(w["nrhs_range"][1])] for lat in lats]
     st0 = srv.stats()
-    dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dist.local_rank)
+    clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     ids, t_sub = [None] * len(reqs), [0.0] * len(reqs)
     t0 = time.perf_counter()
@@ -568,9 +616,7 @@ def run_serve(args, dist: Dist):
     st = srv.stats()
     t_wall = max(t_done) - t0
     solves = sum(len(r[3]) for r in reqs)
-    value = dist.sum(solves / t_wall)
     lat_ms = [1e3 * r.latency_seconds for r in results]
-    ok = all(r.converged for r in results)
     # correctness spot check: a solution through the public API against the FP64 true residual
     g_chk = len(lats) - 1
     rid = srv.submit(gids[g_chk], w["kappa"], [pools[g_chk][0]], w["tol"])
@@ -599,43 +645,63 @@ def run_serve(args, dist: Dist):
         start = max(ta, t_free)
         t_free = start + dt
         lat64.append(1e3 * (t_free - ta))
-    fifo_rate = solves / t_free  # wall rate of the FIFO schedule of this stream
+    for G in gauges:
+        G.close()
+    for lat in lats:
+        lat.close()
     fifo_capacity = solves / busy
-    out = {
-        "metric": "served CG solves/s at 1e-10 residual (Poisson stream, %d lattices)" % len(lats),
-        "value": round(value, 4),
-        "unit": "solves/s", "n_gpus": dist.world, "steps": len(reqs), "warmup": len(lats),
-        "ms_per_step": round(1e3 * t_wall / len(reqs), 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": {"f32": "f32+f64", "f16": "f16+f64"}[args.precision],
-        "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources, Poisson arrivals",
-        "config": {"workload": args.workload, "lattices": ["x".join(map(str, d)) for d in w["lattices"]],
-                   "requests": len(reqs), "rate_per_s": w["rate"], "nrhs_range": w["nrhs_range"],
-                   "kappa_range": w["kappa_range"], "tol": w["tol"], "link_format": args.link_format,
-                   "precision": args.precision, "delta": args.delta, "parallelism": f"replicas{dist.world}"},
-        "e2e": {"value": round(value, 4), "unit": "solves/s", "note": "host arrays in and out through the server",
-                "h2d_bytes_per_step": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs)),
-                "d2h_bytes_per_step": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs))},
+    value = solves / t_wall
+    return {
+        "value": value, "solves": solves, "requests": len(reqs), "wall_s": t_wall, "clocks": clk,
         "latency_ms_p50": pct(lat_ms, 0.5), "latency_ms_p99": pct(lat_ms, 0.99),
         "queue_ms_p50": pct([1e3 * r.queue_seconds for r in results], 0.5),
         "submit_lag_ms_max": round(1e3 * max(ts - (t0 + r[0]) for ts, r in zip(t_sub, reqs)), 3),
-        "all_converged": ok, "max_true_residual": max(r.true_residual for r in results),
-        "spot_check_residual": chk, "solves": solves, "wall_s": round(t_wall, 3),
+        "all_converged": all(r.converged for r in results),
+        "max_true_residual": max(r.true_residual for r in results), "spot_check_residual": chk,
         "speedup_vs_fifo_f64_capacity": round(value / fifo_capacity, 3),
-        "fifo_f64": {"solves_per_s": round(fifo_rate, 3), "capacity_solves_per_s": round(fifo_capacity, 3),
+        "fifo_f64": {"solves_per_s": round(solves / t_free, 3), "capacity_solves_per_s": round(fifo_capacity, 3),
                      "latency_ms_p50": pct(lat64, 0.5), "latency_ms_p99": pct(lat64, 0.99),
                      "all_converged": ok64},
         "server_stats": {k: (round(st[k] - st0[k], 3) if k.startswith("seconds") else st[k])
                          for k in ("completed", "solves_completed", "rejected", "cancelled", "seconds_admit",
                                    "seconds_run", "seconds_retire")},
         "gpu_launches": int(st["kernel_launches"] - st0["kernel_launches"]),
-        "chunks": int(st["chunks"] - st0["chunks"]), "clocks": clk, "impl": "ours",
+        "chunks": int(st["chunks"] - st0["chunks"]),
+        "bytes_per_request": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs)),
+    }
+
+
+def run_serve(args, dist: Dist):
+    """Poisson request stream through the server, and the same stream through the FP64 CG (FIFO)."""
+    import torch
+    import hila_b200 as hw
+    torch.cuda.set_device(dist.local_rank)
+    dist.init("nccl")
+    w = WORKLOADS[args.workload]
+    ctx = hw.Context(dist.local_rank)
+    dist.barrier()
+    m = serve_measure(ctx, w, args, dist.rank)
+    t_wall = dist.max(m["wall_s"])
+    value = dist.sum(m["value"])
+    out = {
+        "metric": "served CG solves/s at 1e-10 residual (Poisson stream, %d lattices)" % len(w["lattices"]),
+        "value": round(value, 4),
+        "unit": "solves/s", "n_gpus": dist.world, "steps": m["requests"], "warmup": len(w["lattices"]),
+        "ms_per_step": round(1e3 * t_wall / m["requests"], 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"f32": "f32+f64", "f16": "f16+f64"}[args.precision],
+        "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources, Poisson arrivals",
+        "config": {"workload": args.workload, "lattices": ["x".join(map(str, d)) for d in w["lattices"]],
+                   "requests": m["requests"], "rate_per_s": w["rate"], "nrhs_range": w["nrhs_range"],
+                   "kappa_range": w["kappa_range"], "tol": w["tol"], "link_format": args.link_format,
+                   "precision": args.precision, "delta": args.delta, "parallelism": f"replicas{dist.world}",
+                   "hbm_budget": "80% of free device memory"},
+        "e2e": {"value": round(value, 4), "unit": "solves/s", "note": "host arrays in and out through the server",
+                "h2d_bytes_per_step": m["bytes_per_request"], "d2h_bytes_per_step": m["bytes_per_request"]},
+        "clocks": m["clocks"], "impl": "ours",
+        **{k: v for k, v in m.items() if k not in ("value", "clocks", "bytes_per_request", "requests")},
     }
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
-    for G in gauges:
-        G.close()
-    for lat in lats:
-        lat.close()
     ctx.close()
     dist.close()
 
@@ -694,7 +760,7 @@ def run_reference(args, dist: Dist):
     out = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": dist.world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-           "config": {"workload": args.workload, "lattice": "x".join(map(str, w["dims"])), "kappa": w["kappa"]},
+           "config": workload_config(args, w, dist.world),
            "cpu_baseline": {"value": value, "unit": unit, "cores": cs["cores"], "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -712,6 +778,7 @@ def main():
     ap.add_argument("--link-format", type=int, default=12, choices=[18, 12])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="CG iterations from a host loop (for launch lists)")
+    ap.add_argument("--no-served", action="store_true", help="mrhs: skip the served (serve32) comparison")
     ap.add_argument("--delta", type=float, default=None,
                     help="reliable-update factor of the mixed-precision solves (default 0.005 FP16, 1e-5 FP32)")
     ap.add_argument("--lattice", default=None, help="override the workload's lattice, e.g. 24x24x24x24")

@@ -85,7 +85,8 @@ class _RequestResult(ctypes.Structure):
 
 
 class _EngineProfile(ctypes.Structure):
-    _fields_ = [("launches", ctypes.c_int * 12), ("ms", ctypes.c_double * 12)]
+    _fields_ = [("launches", ctypes.c_int * 12), ("ms", ctypes.c_double * 12),
+                ("work", (ctypes.c_uint64 * 4) * 12)]
 
 
 class _ServerStats(ctypes.Structure):
@@ -299,10 +300,15 @@ class Context:
         _check(lib().hw_engine_profile_enable(self.handle, int(bool(enable))))
 
     def engine_profile_get(self, precision: str = "f16") -> dict:
-        """{phase: (launches with work, summed ms)} of one engine (hw_engine_profile_get)."""
+        """{phase: (launches with work, summed ms, work units)} of one engine (hw_engine_profile_get).
+
+        The work units are the four counters of ``hw_engine_profile.work`` (sites x solves of
+        the main form, of the alternate form, sites whose links were read, R3 of the normal
+        system); multiplied by the bytes of each unit they give the algorithmic bytes."""
         out = _EngineProfile()
         _check(lib().hw_engine_profile_get(self.handle, PRECISIONS[precision], ctypes.byref(out)))
-        return {name: (out.launches[k], out.ms[k]) for k, name in enumerate(self.ENGINE_PHASES)}
+        return {name: (out.launches[k], out.ms[k], tuple(int(v) for v in out.work[k]))
+                for k, name in enumerate(self.ENGINE_PHASES)}
 
     def stream(self) -> int:
         """The library's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

@@ -55,6 +55,7 @@ Engine::~Engine() {
     if (chunk_exec_) cudaGraphExecDestroy(chunk_exec_);
     if (pinned_states_) cudaFreeHost(pinned_states_);
     if (pinned_ctl_) cudaFreeHost(pinned_ctl_);
+    if (pinned_work_) cudaFreeHost(pinned_work_);
     for (cudaEvent_t e : prof_ev_)
         if (e) cudaEventDestroy(e);
 }
@@ -66,10 +67,14 @@ int Engine::init() {
     if ((rc = d_states_.alloc(sizeof(EngState) * kEngMaxProb)) != HW_OK) return rc;
     if ((rc = d_tickets_.alloc(sizeof(unsigned) * kEngMaxLat)) != HW_OK) return rc;
     if ((rc = d_ctl_.alloc(sizeof(int) * 8)) != HW_OK) return rc;
+    if ((rc = d_work_.alloc(sizeof(unsigned long long) * kEngPhases * kEngWorkKinds)) != HW_OK) return rc;
     HW_CUDA(cudaMemsetAsync(d_tickets_.ptr, 0, d_tickets_.bytes, ctx_->stream));
     HW_CUDA(cudaMemsetAsync(d_ctl_.ptr, 0, d_ctl_.bytes, ctx_->stream));
+    HW_CUDA(cudaMemsetAsync(d_work_.ptr, 0, d_work_.bytes, ctx_->stream));
     HW_CUDA(cudaMallocHost(&pinned_states_, sizeof(EngState) * kEngMaxProb));
     HW_CUDA(cudaMallocHost(&pinned_ctl_, sizeof(int) * 8));
+    HW_CUDA(cudaMallocHost(&pinned_work_, d_work_.bytes));
+    std::memset(pinned_work_, 0, d_work_.bytes);
     std::memset(&tables_, 0, sizeof(tables_));
     for (int j = 0; j < kEngMaxProb; j++) {
         std::memset(&host_states_[j], 0, sizeof(EngState));
@@ -332,6 +337,7 @@ void Engine::set_ptrs() {
     ptrs_.partials = d_partials_.as<double>();
     ptrs_.tickets = d_tickets_.as<unsigned>();
     ptrs_.ctl = d_ctl_.as<int>();
+    ptrs_.work = d_work_.as<unsigned long long>();
 }
 
 int Engine::build_graph() {
@@ -373,8 +379,10 @@ int Engine::configure() {
     if (mask == 0) mask = 1;
     int variant = default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
-    // the tensor-core variant reads the 18-real FP16 links, which exist only with full18_
-    if (variant < 0 || variant > 7 || (variant == 4 && (low_ != LOW_F16 || !full18_))) variant = default_variant();
+    // launch shapes (engine.cu): 2 for both precisions, 4 and 7 for FP16 only; the
+    // tensor-core variant 4 reads the 18-real FP16 links, which exist only with full18_
+    const bool known = variant == 2 || (low_ == LOW_F16 && (variant == 7 || (variant == 4 && full18_)));
+    if (!known) variant = default_variant();
     if (variant != grid_.variant || mask != grid_.planes_mask) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
         if (chunk_exec_) {
@@ -410,37 +418,41 @@ int Engine::launch_chunk(int iters) {
 }
 
 // Host-loop chunk with events around every phase; synchronises after each
-// iteration to attribute its phase times (P1..P4 count when some running slot
-// had no reliable update pending, R1..R5 when some slot made one, P5 when some
-// slot was running).
+// iteration to attribute its phase times.  A phase launch counts when its work
+// units (engine.h) grew: launches that found no active slot are left out.
 int Engine::launch_chunk_profiled(int iters) {
     for (cudaEvent_t &e : prof_ev_)
         if (!e) HW_CUDA(cudaEventCreate(&e));
     set_ptrs();
     eng_enqueue_chunk_begin(ptrs_, ctx_->stream);
+    // the counters as they are now (launches outside profiling also count)
+    HW_CUDA(cudaMemcpyAsync(pinned_work_, d_work_.ptr, d_work_.bytes, cudaMemcpyDeviceToHost, ctx_->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx_->stream));
     for (int k = 0; k < iters; k++) {
-        int running = 0, inner = 0, ru_before = 0, ru_after = 0;
+        int running = 0;
         for (int j = 0; j < kEngMaxProb; j++)
-            if (slots_[j].used) {
-                running += host_states_[j].status == ENG_RUNNING;
-                inner += host_states_[j].status == ENG_RUNNING && host_states_[j].ru == 0;
-                ru_before += host_states_[j].n_ru;
-            }
+            if (slots_[j].used) running += host_states_[j].status == ENG_RUNNING;
         if (running == 0) break;
+        std::memcpy(work_seen_, pinned_work_, sizeof(work_seen_));
         eng_enqueue_iteration(low_, ptrs_, grid_, ctx_->stream, prof_ev_);
         eng_enqueue_control(ptrs_, kEngMaxProb, iters, 0, 0, ctx_->stream);
         int rc;
         if ((rc = read_states()) != HW_OK) return rc;
-        for (int j = 0; j < kEngMaxProb; j++)
-            if (slots_[j].used) ru_after += host_states_[j].n_ru;
         for (int ph = 0; ph < kEngPhases; ph++) {
-            const bool ru_phase = eng_ru_phase(ph);
-            if (ru_phase && ru_after == ru_before) continue;
-            if (ph <= PH_P4 && inner == 0) continue;
+            bool did = false;
+            for (int w = 0; w < kEngWorkKinds; w++) {
+                const int q = ph * kEngWorkKinds + w;
+                did |= pinned_work_[q] != work_seen_[q];
+            }
+            if (!did) continue;
             float ms = 0.f;
             HW_CUDA(cudaEventElapsedTime(&ms, prof_ev_[ph], prof_ev_[ph + 1]));
             prof_ms_[ph] += ms;
             prof_n_[ph] += 1;
+            for (int w = 0; w < kEngWorkKinds; w++) {
+                const int q = ph * kEngWorkKinds + w;
+                prof_work_[q] += pinned_work_[q] - work_seen_[q];
+            }
         }
     }
     HW_CUDA(cudaGetLastError());
@@ -452,19 +464,22 @@ void Engine::reset_profile() {
         prof_n_[ph] = 0;
         prof_ms_[ph] = 0.0;
     }
+    std::memset(prof_work_, 0, sizeof(prof_work_));
 }
 
-void Engine::profile(int *launches, double *ms) const {
+void Engine::profile(int *launches, double *ms, unsigned long long *work) const {
     for (int ph = 0; ph < kEngPhases; ph++) {
         launches[ph] = (int)prof_n_[ph];
         ms[ph] = prof_ms_[ph];
     }
+    std::memcpy(work, prof_work_, sizeof(prof_work_));
 }
 
 int Engine::read_states() {
     HW_CUDA(cudaMemcpyAsync(pinned_states_, d_states_.ptr, sizeof(EngState) * kEngMaxProb, cudaMemcpyDeviceToHost,
                             ctx_->stream));
     HW_CUDA(cudaMemcpyAsync(pinned_ctl_, d_ctl_.ptr, sizeof(int) * 8, cudaMemcpyDeviceToHost, ctx_->stream));
+    HW_CUDA(cudaMemcpyAsync(pinned_work_, d_work_.ptr, d_work_.bytes, cudaMemcpyDeviceToHost, ctx_->stream));
     HW_CUDA(cudaStreamSynchronize(ctx_->stream));
     HW_CUDA(cudaGetLastError());
     bodies_total_ = reinterpret_cast<const unsigned long long *>(pinned_ctl_ + 6)[0];

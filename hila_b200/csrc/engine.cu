@@ -90,6 +90,13 @@ __device__ __forceinline__ void stc(double2 *p, int stride, int c, int i, Cx<dou
 
 static_assert(kEngMaxRhs <= 32, "one warp lane per slot of a lattice");
 
+// Work units of a phase launch (engine.h, kEngWorkKinds).  Called once per lattice and
+// launch (by the block that meets the lattice's first tile), with every site of the
+// lattice counted: all tiles of a lattice see the same active slots.
+__device__ __forceinline__ void count_work(const EngPtrs &P, int phase, int kind, unsigned long long units) {
+    if (units) atomicAdd(P.work + phase * kEngWorkKinds + kind, units);
+}
+
 // Active slots of every lattice for one phase launch, built once per block: slot
 // states change only in the finishers, and a lattice's finisher runs after all of
 // its work items, so the table stays valid for every item the block still meets.
@@ -406,6 +413,10 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
         }
         __syncthreads();
         const int na = s_na;
+        if (lt == 0 && threadIdx.x == 0 && na > 0) {
+            count_work(P, PHASE, 0, (unsigned long long)na * g.Vh);
+            count_work(P, PHASE, 2, g.Vh);
+        }
         SiteNbrs nb;
         if (valid && na > 0) nb = site_neighbours(g, i, OUTPAR);
         const LinksF16x18Smem<kEngTile> US{s_lx, s_lz, OUTPAR};
@@ -522,6 +533,21 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
         const int lt = tile - La.tile0;
         const int i = lt * kEngTile + threadIdx.x;
         const EngProblem &pr = T->prob[j];
+        if (lt == 0 && threadIdx.x == 0) {
+            // R3 of a first update from x = 0 runs no hop (below); the links are read
+            // once per site when some slot of the lattice runs its hop
+            const bool nohop = PHASE == PH_R3 && P.S[j].init && !P.S[j].xnz;
+            const int kind = (PHASE == PH_R3 && pr.mode == ENG_MODE_NORMAL) ? 3 : (nohop ? 1 : 0);
+            count_work(P, PHASE, kind, (unsigned long long)g.Vh);
+            if (a == 0) {
+                bool hop = false;
+                for (int q = 0; q < na; q++) {
+                    const EngState &sq = P.S[act.slot[l][q]];
+                    hop |= !(PHASE == PH_R3 && sq.init && !sq.xnz);
+                }
+                if (hop) count_work(P, PHASE, 2, (unsigned long long)g.Vh);
+            }
+        }
         double red[2] = {0.0, 0.0};
         if (i < g.Vh) {
             const SiteNbrs nb = site_neighbours(g, i, OUTPAR);
@@ -574,6 +600,10 @@ __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
             const EngState &s = P.S[j];
             if (!active<PHASE>(s)) continue;
             const EngProblem &pr = T->prob[j];
+            if (i == 0) {
+                const bool alt = PHASE == PH_R1 ? pr.mode == ENG_MODE_NORMAL : s.init != 0;
+                count_work(P, PHASE, alt ? 1 : 0, (unsigned long long)La.g.Vh);
+            }
             if (PHASE == PH_R1) {
                 SpinorF32 ys{pr.y, stride};
                 Spinor<float> y;
@@ -796,45 +826,26 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 }
 
 // Launch shapes of the low-precision phases (EngGrid::variant):
-//   0: one right-hand side per thread, <= 128 registers (4 blocks of 128 per SM)
-//   1: one right-hand side per thread, <= 102 registers (5 blocks)
-//   2: one right-hand side per thread, <= 85 registers (6 blocks)
-//   3: two right-hand sides per thread sharing the links, <= 128 registers
+//   2: one right-hand side per thread, <= 85 registers (6 blocks of 128 per SM); the FP32 default
 //   4: FP16 only: the hop as tensor-core products over groups of sources (engine_mma.cuh)
-//   5: FP16: two right-hand sides per thread in the lanes of packed FP32
-//      instructions (pair.cuh), <= 128 registers, every inner phase
-//   6, 7: P1, P3 packed as in 5 with <= 128 / 168 registers (4 / 3 blocks), P2, P4 and
-//      the reliable update as variant 2 (FP32 input falls back to variant 3's hop)
-// variants 0-3 with the inner links either 18-real FP32 (G.full18) or the precision's 12-real format
+//   7: FP16 only, the default: P1, P3 with two right-hand sides per thread in the lanes of
+//      packed FP32 instructions (pair.cuh), <= 168 registers (3 blocks); P2, P4 and the
+//      reliable update as variant 2
+// (one right-hand side per thread at 4 or 5 blocks per SM, two per thread sharing the links
+// without packing, and packed P1..P4 were measured slower and removed)
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
-    if (LOW == LOW_F16 && G.variant == 4) {
-        enqueue_iteration_mma(P, G, s, ev);
-        return;
+    if constexpr (LOW == LOW_F16) {
+        if (G.variant == 4) {
+            enqueue_iteration_mma(P, G, s, ev);
+            return;
+        }
+        if (G.variant == 7) {
+            enqueue_iteration_hybrid<LOW, 3, FULL18>(P, G, s, ev);
+            return;
+        }
     }
-    switch (G.variant) {
-    case 1:
-        enqueue_iteration_t<LOW, 1, 5, FULL18>(P, G, s, ev);
-        break;
-    case 2:
-        enqueue_iteration_t<LOW, 1, 6, FULL18>(P, G, s, ev);
-        break;
-    case 3:
-        enqueue_iteration_t<LOW, 2, 4, FULL18>(P, G, s, ev);
-        break;
-    case 5:
-        enqueue_iteration_t<LOW, 2, 4, FULL18, true>(P, G, s, ev);
-        break;
-    case 6:
-        enqueue_iteration_hybrid<LOW, 4, FULL18>(P, G, s, ev);
-        break;
-    case 7:
-        enqueue_iteration_hybrid<LOW, 3, FULL18>(P, G, s, ev);
-        break;
-    default:
-        enqueue_iteration_t<LOW, 1, 4, FULL18>(P, G, s, ev);
-        break;
-    }
+    enqueue_iteration_t<LOW, 1, 6, FULL18>(P, G, s, ev);
 }
 
 template <int LOW>
@@ -881,20 +892,7 @@ int occupancy_variant(int v) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_eng_mma<PH_P4, kMmaMinBlocks>, kEngTile, 0);
         return n < 1 ? 1 : n;
     }
-    switch (v) {
-    case 1:
-        return occupancy_low<LOW, 1, 5>();
-    case 2:
-    case 6:
-    case 7:
-        return occupancy_low<LOW, 1, 6>();
-    case 3:
-        return occupancy_low<LOW, 2, 4>();
-    case 5:
-        return occupancy_low<LOW, 2, 4, true>();
-    default:
-        return occupancy_low<LOW, 1, 4>();
-    }
+    return occupancy_low<LOW, 1, 6>();
 }
 
 EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask) {
@@ -906,13 +904,7 @@ EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask) {
     EngGrid G;
     G.low = sms * lo;
     G.pk = G.low;
-    if (variant == 6 || variant == 7) {
-        const int pk = low == LOW_F16 ? (variant == 6 ? occupancy_low<LOW_F16, 2, 4, true, PH_P1>()
-                                                       : occupancy_low<LOW_F16, 2, 3, true, PH_P1>())
-                                      : (variant == 6 ? occupancy_low<LOW_F32, 2, 4, true, PH_P1>()
-                                                       : occupancy_low<LOW_F32, 2, 3, true, PH_P1>());
-        G.pk = sms * pk;
-    }
+    if (variant == 7 && low == LOW_F16) G.pk = sms * occupancy_low<LOW_F16, 2, 3, true, PH_P1>();
     G.f64 = sms * (hi < 1 ? 1 : hi);
     G.variant = variant;
     G.full18 = full18;

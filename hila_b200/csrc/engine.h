@@ -111,7 +111,18 @@ struct EngPtrs {
     int *ctl;             // [0] iterations run in this chunk, [1] running slots,
                           // [2] reliable updates requested in this iteration,
                           // [3] iteration limit of a chunk (control kernel with chunk <= 0)
+    unsigned long long *work;  // kEngPhases x kEngWorkKinds cumulative work units (below)
 };
+
+// Work units counted by every phase launch (cumulative, per phase), from which the
+// algorithmic bytes of the launches that did work follow:
+//   [0] sites x slots that ran the phase's main form
+//   [1] sites x slots of its alternate form: R1 normal-system slots (y also cleared),
+//       R3 solve-mode slots of a first update from x = 0 (no hop), P5 first iterations
+//       (p = r, p not read)
+//   [2] sites whose links were read (once per site and launch, shared by the slots)
+//   [3] R3: sites x slots of the normal system (s = M x in FP64)
+constexpr int kEngWorkKinds = 4;
 
 struct EngGrid {
     int low;  // blocks of the low-precision phases (all SMs x resident blocks)

@@ -49,10 +49,11 @@ class Engine {
     int read_states();
     // loop bodies (10 phase kernels + 1 control kernel each) run since init, as of the last read_states
     unsigned long long bodies_total() const { return bodies_total_; }
-    // per-phase device time of the iterations that had work in that phase, while the
-    // context's engine profiling is on (iterations then run from a synchronising host loop)
+    // per-phase device time and work units (engine.h, kEngWorkKinds) of the launches
+    // that did work, while the context's engine profiling is on (iterations then run
+    // from a synchronising host loop)
     void reset_profile();
-    void profile(int *launches, double *ms) const;
+    void profile(int *launches, double *ms, unsigned long long *work) const;
     const EngState &state(int slot) const { return host_states_[slot]; }
     void release(int slot);
     int nslots_used() const;
@@ -82,12 +83,15 @@ class Engine {
     EngState host_states_[kEngMaxProb];
     EngState *pinned_states_ = nullptr;
     int *pinned_ctl_ = nullptr;
+    unsigned long long *pinned_work_ = nullptr;  // kEngPhases x kEngWorkKinds, as of the last read_states
+    unsigned long long work_seen_[kEngPhases * kEngWorkKinds] = {};
+    unsigned long long prof_work_[kEngPhases * kEngWorkKinds] = {};
     unsigned long long bodies_total_ = 0;
     cudaEvent_t prof_ev_[kEngPhases + 1] = {};
     long prof_n_[kEngPhases] = {};
     double prof_ms_[kEngPhases] = {};
     int launch_chunk_profiled(int iters);
-    DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_;
+    DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_, d_work_;
     size_t partial_tiles_ = 0;
     EngGrid grid_{};
     EngPtrs ptrs_{};

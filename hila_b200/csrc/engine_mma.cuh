@@ -279,6 +279,10 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_mma(EngPtrs P) {
         if (lane < kEngMaxRhs) W.acc[lane] = 0.0;
         __syncthreads();
         const int na = s_na;
+        if (lt == 0 && threadIdx.x == 0 && na > 0) {
+            count_work(P, PHASE, 0, (unsigned long long)na * La.g.Vh);
+            count_work(P, PHASE, 2, La.g.Vh);
+        }
         const int site0 = lt * kEngTile + warp * 32;
         for (int rg = 0; rg < na;) {
             const int left = na - rg;

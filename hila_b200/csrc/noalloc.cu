@@ -68,17 +68,19 @@ extern "C" int hw_wilson_evenodd_apply_noalloc(const int dims[4], int t_antiperi
                                                const double *links, int link_format, const double *in_even,
                                                double *out_even, int stride, void *stream) {
     HW_CHECK_ARG(dims && links && in_even && out_even, "null argument");
+    // the running product is checked after every factor, so it never exceeds
+    // 2 * kNoAllocMaxSites * 2^31 and cannot overflow
     long V = 1;
     for (int d = 0; d < 4; d++) {
         HW_CHECK_ARG(dims[d] >= 2 && dims[d] % 2 == 0, "dims[%d] = %d: every extent must be even and >= 2", d,
                      dims[d]);
         V *= dims[d];
+        HW_CHECK_ARG(V <= 2L * kNoAllocMaxSites,
+                     "lattice has more than %d sites per parity; the allocation-free operator supports at most "
+                     "%d (a 16^4 lattice) -- use hw_wilson_evenodd_apply",
+                     kNoAllocMaxSites, kNoAllocMaxSites);
     }
     const long Vh = V / 2;
-    HW_CHECK_ARG(Vh <= kNoAllocMaxSites,
-                 "lattice has %ld sites per parity; the allocation-free operator supports at most %d "
-                 "(a 16^4 lattice) -- use hw_wilson_evenodd_apply",
-                 Vh, kNoAllocMaxSites);
     HW_CHECK_ARG(stride >= Vh, "stride %d is smaller than the %ld sites per parity", stride, Vh);
     HW_CHECK_ARG(sign == 1 || sign == -1, "sign must be +1 (apply) or -1 (dagger)");
     HW_CHECK_ARG(link_format == 18 || link_format == 12, "link_format must be 18 or 12");

@@ -184,7 +184,8 @@ int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     std::memset(out, 0, sizeof(*out));
     static_assert(HW_ENGINE_PHASES == kEngPhases, "phase count");
-    if (Engine *e = ctx->engines[low_of(precision)]) e->profile(out->launches, out->ms);
+    static_assert(HW_ENGINE_WORK_KINDS == kEngWorkKinds, "work kinds");
+    if (Engine *e = ctx->engines[low_of(precision)]) e->profile(out->launches, out->ms, &out->work[0][0]);
     return HW_OK;
 }
 

@@ -358,9 +358,19 @@ int hw_staggered_cg_solve(const hw_gauge *gauge, double mass, const hw_stag_fiel
  * r = M^dag s by R4, R5 (FP64, normal system) or R4L, R5L (low precision,
  * M x = b); P5 p = r + beta p. */
 #define HW_ENGINE_PHASES 12
+/* Work units of a phase, summed over its launches that had work:
+ *   [0] sites x solves that ran the phase's main form;
+ *   [1] sites x solves of its alternate form: R1 of a normal-equation solve (y also
+ *       cleared), R3 of a first reliable update from x = 0 (no hop), P5 of a first
+ *       iteration (p = r, p not read);
+ *   [2] sites whose links the launch read (once per site, shared by the solves);
+ *   [3] R3 of a normal-equation solve (s = M x stored in FP64).
+ * Multiplied by the bytes each unit moves they give a launch's algorithmic bytes. */
+#define HW_ENGINE_WORK_KINDS 4
 typedef struct hw_engine_profile {
     int launches[HW_ENGINE_PHASES]; /* launches that had work */
     double ms[HW_ENGINE_PHASES];    /* their summed device time */
+    unsigned long long work[HW_ENGINE_PHASES][HW_ENGINE_WORK_KINDS];
 } hw_engine_profile;
 /* enabling resets the counters of the context's engines */
 int hw_engine_profile_enable(hw_context *ctx, int enable);

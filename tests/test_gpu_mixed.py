@@ -156,3 +156,32 @@ def test_batch_refills_slots(hw, ctx, oracle):
     for (D, fb, fx, _), b, r in zip(reqs, bs, results):
         assert r.converged
         assert oracle.true_residual(dims, U, D.kappa, b, fx.download()) <= TOL
+
+
+@pytest.mark.parametrize("variant", [2, 4, 7])
+def test_engine_launch_shapes(hw, ctx, oracle, variant, monkeypatch):
+    """Every launch shape the FP16 engine keeps (HW_ENGINE_VARIANT: 2 one source per thread,
+    4 the tensor-core hop, 7 the packed default): a batch of three sources on two lattices
+    converges to true residual 1e-10 by the oracle, and each solve is bitwise the same alone
+    as in the batch.  The shapes differ in how products are rounded, so solutions of
+    different shapes are compared only through the true residual."""
+    monkeypatch.setenv("HW_ENGINE_VARIANT", str(variant))
+    specs = [((8, 8, 8, 8), 81, 0.124), ((4, 4, 4, 8), 82, 0.12)]
+    built = []
+    for dims, seed, kappa in specs:
+        U, lat, G = make(hw, ctx, oracle, dims, seed)
+        built.append((dims, U, lat, hw.Dirac_Wilson_evenodd(kappa, G), kappa))
+    work = []
+    for n, (dims, U, lat, D, kappa) in enumerate(built):
+        for k in range(2 if n == 0 else 1):
+            b = oracle.gen_spinor(dims, 90 + 10 * n + k, oracle.EVEN)
+            work.append((dims, U, lat, D, kappa, b, hw.Field(lat, b), hw.Field(lat)))
+    res = hw.batch_solve(ctx, [(D, fb, fx, TOL) for (_, _, _, D, _, _, fb, fx) in work], precision="f16")
+    for (dims, U, lat, D, kappa, b, fb, fx), r in zip(work, res):
+        assert r.converged, (variant, r)
+        x = fx.download()
+        assert oracle.true_residual(dims, U, kappa, b, x) <= TOL
+        alone = hw.Field(lat)
+        [ra] = hw.batch_solve(ctx, [(D, fb, alone, TOL)], precision="f16")
+        assert ra.iterations == r.iterations
+        assert np.array_equal(alone.download(), x), variant
