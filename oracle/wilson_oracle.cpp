@@ -32,12 +32,16 @@
 // (applications/test_cases/test_CG.cpp:236-245) asserts they are.  The oracle
 // implements the intended term  E_{mu,-s}( U_mu(x-mu)^dagger P_{mu,-s} psi(x-mu) ).
 //
-// Parity of this oracle is pinned by the reference's own identity tests
+// Parity of this oracle is pinned against golden vectors made by the reference's
+// own code: oracle/ref_pin compiles the reference's site algebra (Complex, Matrix,
+// SU(N), HalfWilsonVector projection / expand, gamma matrices) and its generators
+// with g++, and tests/golden/ref_wilson.npz holds their outputs (links, sources,
+// even-odd apply and dagger, hop, single-site tables; tests/test_ref_golden.py).
+// The reference's applications cannot be built here (hilapp needs LLVM/Clang and
+// the Wilson headers are bit-rotted), so the CG is pinned by its identity tests
 // (test_CG.cpp: gamma identities, adjointness, CG identities) re-run on random
 // links, by an independent numpy restatement with explicit 4x4 gamma matrices,
-// and by the analytic free-field plane-wave spectrum.  The reference itself
-// cannot be compiled here (hilapp needs LLVM/Clang, MPI headers are absent and
-// the Wilson headers are bit-rotted) and ships no golden vectors for this path.
+// and by the analytic free-field plane-wave spectrum.
 //
 // Host data layouts (the canonical exchange layout of the C ABI as well):
 //   spinor field : psi[V][4 spin][3 colour] complex double, lexicographic
