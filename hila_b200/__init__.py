@@ -81,7 +81,8 @@ class _ServerConfig(ctypes.Structure):
 class _RequestResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("nrhs", ctypes.c_int), ("iterations", ctypes.c_int),
                 ("reliable_updates", ctypes.c_int), ("true_residual", ctypes.c_double),
-                ("latency_seconds", ctypes.c_double), ("queue_seconds", ctypes.c_double)]
+                ("latency_seconds", ctypes.c_double), ("queue_seconds", ctypes.c_double),
+                ("admit_chunk", ctypes.c_uint64), ("retire_chunk", ctypes.c_uint64)]
 
 
 class _EngineProfile(ctypes.Structure):
@@ -128,6 +129,8 @@ _SIGNATURES = {
     "hw_field_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "hw_field_destroy": (ctypes.c_int, [_vp]),
     "hw_field_upload": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_field_upload_eo": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_field_download_eo": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "hw_field_download": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "hw_field_zero": (ctypes.c_int, [_vp, ctypes.c_int]),
     "hw_wilson_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
@@ -168,6 +171,12 @@ _SIGNATURES = {
                                         ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "hw_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.POINTER(_dp), ctypes.c_double,
                                       ctypes.POINTER(_RequestResult)]),
+    "hw_server_submit_eo": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_dp),
+                                           ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+    "hw_server_submit_fields": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                               ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_double,
+                                               ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "hw_server_cancel": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "hw_server_stats_get": (ctypes.c_int, [_vp, ctypes.POINTER(_ServerStats)]),
     "hw_generate_links": (ctypes.c_int, [_ip, ctypes.c_double, ctypes.c_uint64, _dp]),
@@ -239,6 +248,16 @@ def generate_spinor(dims, seed: int, parity: int = ALL) -> np.ndarray:
     psi = np.empty((V, 4, 3, 2), np.float64)
     _check(lib().hw_generate_spinor(_dims(dims), int(seed), int(parity), _dptr(psi)))
     return psi
+
+
+def eo_order(dims) -> np.ndarray:
+    """Lexicographic site index of each position of HILA's even-first site order
+    (lattice.cpp:171-184): EVEN sites in increasing lexicographic order, then ODD.
+    `lex_array[eo_order(dims)]` is the array in even-first order."""
+    Lx, Ly, Lz, Lt = dims
+    lex = np.arange(Lx * Ly * Lz * Lt)
+    par = (lex % Lx + (lex // Lx) % Ly + (lex // (Lx * Ly)) % Lz + lex // (Lx * Ly * Lz)) % 2
+    return np.concatenate([lex[par == 0], lex[par == 1]])
 
 
 class PinnedArray:
@@ -409,6 +428,23 @@ class Field:
         if out is None:
             out = np.zeros((self.lattice.volume, 4, 3, 2), np.float64)
         _check(lib().hw_field_download(self.handle, _dptr(out), int(parity)))
+        return out
+
+    def upload_eo(self, data: np.ndarray, parity: int = ALL):
+        """hw_field_upload_eo: `data` in even-first site order ((V,4,3,2), EVEN sites first);
+        only the sites of `parity` are copied."""
+        if data.dtype != np.float64 or not data.flags.c_contiguous or data.size != self.lattice.volume * 24:
+            raise ValueError("spinor arrays hold V*24 contiguous doubles")
+        _check(lib().hw_field_upload_eo(self.handle, _dptr(data), int(parity)))
+
+    def download_eo(self, parity: int = ALL, out: np.ndarray | None = None) -> np.ndarray:
+        """hw_field_download_eo: the sites of `parity` into `out` in even-first site order; the
+        other parity of `out` is left as it is."""
+        if out is None:
+            out = np.zeros((self.lattice.volume, 4, 3, 2), np.float64)
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.lattice.volume * 24:
+            raise ValueError("spinor arrays hold V*24 contiguous doubles")
+        _check(lib().hw_field_download_eo(self.handle, _dptr(out), int(parity)))
         return out
 
     def zero(self, parity: int = ALL):
@@ -712,6 +748,8 @@ class RequestResult:
     true_residual: float
     latency_seconds: float
     queue_seconds: float
+    admit_chunk: int = 0
+    retire_chunk: int = 0
 
     @property
     def converged(self) -> bool:
@@ -773,6 +811,30 @@ class Server:
                                       int(maxiters), ctypes.byref(rid)))
         return rid.value
 
+    def submit_eo(self, gauge_id: int, kappa: float, sources, solutions, accuracy: float = 1e-10,
+                  maxiters: int = 10000) -> int:
+        """hw_server_submit_eo: host arrays in even-first site order ((V,4,3,2), EVEN sites first).
+        Page-locked arrays (PinnedArray) are copied by DMA directly; keep every array alive and
+        untouched until wait() returns, which also fills pageable solutions."""
+        for a in list(sources) + list(solutions):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        src = (_dp * len(sources))(*[_dptr(a) for a in sources])
+        sol = (_dp * len(solutions))(*[_dptr(a) for a in solutions])
+        rid = ctypes.c_uint64()
+        _check(lib().hw_server_submit_eo(self.handle, int(gauge_id), float(kappa), len(sources), src, sol,
+                                         float(accuracy), int(maxiters), ctypes.byref(rid)))
+        return rid.value
+
+    def submit_fields(self, gauge_id: int, kappa: float, sources, solutions, accuracy: float = 1e-10,
+                      maxiters: int = 10000) -> int:
+        """hw_server_submit_fields: device Fields; the solution fields hold the initial guess."""
+        src = (_vp * len(sources))(*[f.handle for f in sources])
+        sol = (_vp * len(solutions))(*[f.handle for f in solutions])
+        rid = ctypes.c_uint64()
+        _check(lib().hw_server_submit_fields(self.handle, int(gauge_id), float(kappa), len(sources), src, sol,
+                                             float(accuracy), int(maxiters), ctypes.byref(rid)))
+        return rid.value
+
     def wait(self, request_id: int, nrhs: int, volume: int, timeout: float = -1.0, copy: bool = True):
         """Returns (solutions, RequestResult); solutions is a list of (V,4,3,2)
         arrays, or None with copy=False."""
@@ -785,7 +847,7 @@ class Server:
         if rc not in (HW_OK, HW_ERR_CANCELLED, HW_ERR_REJECTED):
             _check(rc)
         return sols, RequestResult(r.status, r.nrhs, r.iterations, r.reliable_updates, r.true_residual,
-                                   r.latency_seconds, r.queue_seconds)
+                                   r.latency_seconds, r.queue_seconds, r.admit_chunk, r.retire_chunk)
 
     def cancel(self, request_id: int) -> None:
         _check(lib().hw_server_cancel(self.handle, ctypes.c_uint64(request_id)))

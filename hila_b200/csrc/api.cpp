@@ -337,6 +337,48 @@ int hw_field_download(const hw_field *f, double *host, int parity) {
     return HW_OK;
 }
 
+int hw_field_upload_eo(hw_field *f, const double *host, int parity) {
+    HW_CHECK_ARG(f && host, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_lattice *lat = f->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    const size_t half = (size_t)lat->Vh * 24;
+    int rc;
+    if ((rc = ensure_stage(ctx, half * sizeof(double))) != HW_OK) return rc;
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) {
+            HW_CUDA(cudaMemcpyAsync(ctx->stage.ptr, host + p * half, half * sizeof(double), cudaMemcpyHostToDevice,
+                                    ctx->stream));
+            launch_aos_to_soa((int)lat->Vh, ctx->stage.as<double>(), f->half[p].h(), ctx->stream);
+        }
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
+int hw_field_download_eo(const hw_field *f, double *host, int parity) {
+    HW_CHECK_ARG(f && host, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_lattice *lat = f->lat;
+    hw_context *ctx = lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    const size_t half = (size_t)lat->Vh * 24;
+    int rc;
+    if ((rc = ensure_stage(ctx, half * sizeof(double))) != HW_OK) return rc;
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) {
+            launch_soa_to_aos((int)lat->Vh, f->half[p].h(), ctx->stage.as<double>(), ctx->stream);
+            HW_CUDA(cudaMemcpyAsync(host + p * half, ctx->stage.ptr, half * sizeof(double), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+        }
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
 int hw_field_zero(hw_field *f, int parity) {
     HW_CHECK_ARG(f, "null argument");
     HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");

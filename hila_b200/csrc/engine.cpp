@@ -381,7 +381,8 @@ int Engine::configure() {
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
     // launch shapes (engine.cu): 2 for both precisions, 4 and 7 for FP16 only; the
     // tensor-core variant 4 reads the 18-real FP16 links, which exist only with full18_
-    const bool known = variant == 2 || (low_ == LOW_F16 && (variant == 7 || (variant == 4 && full18_)));
+    const bool known =
+        variant == 2 || (low_ == LOW_F16 && (variant == 7 || (variant == 4 && full18_)));
     if (!known) variant = default_variant();
     if (variant != grid_.variant || mask != grid_.planes_mask) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);

@@ -8,6 +8,7 @@
 // a solve gives bitwise the same result alone and inside any batch.
 #include <cuda_fp16.h>
 
+#include <mutex>
 #include <type_traits>
 
 #include "engine.h"
@@ -832,7 +833,8 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 //      packed FP32 instructions (pair.cuh), <= 168 registers (3 blocks); P2, P4 and the
 //      reliable update as variant 2
 // (one right-hand side per thread at 4 or 5 blocks per SM, two per thread sharing the links
-// without packing, and packed P1..P4 were measured slower and removed)
+// without packing, packed P1..P4, packed P1..P3, and P1/P3 streaming their neighbour data
+// through a cp.async ring in shared memory were measured slower or no faster and removed)
 template <int LOW, bool FULL18>
 void enqueue_iteration_v(const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
     if constexpr (LOW == LOW_F16) {

@@ -37,6 +37,23 @@ using Clock = std::chrono::steady_clock;
 
 enum ReqState { REQ_QUEUED, REQ_RUNNING, REQ_DONE };
 
+// where a request's sources come from and its solutions go
+enum ReqMode {
+    REQ_HOST_LEX,  // host arrays in lexicographic site order (EVEN sites gathered at submit)
+    REQ_HOST_EO,   // host arrays in even-first site order: the EVEN half is one contiguous block
+    REQ_FIELDS     // device fields: the engine reads b and writes x in place
+};
+
+// page-locked host memory (cudaHostAlloc or cudaHostRegister): copied by DMA directly
+bool host_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // Recycled page-locked host buffers, so source and solution copies run
 // asynchronously at full PCIe rate (page-locking memory per request would
 // cost more than the copy).
@@ -92,7 +109,19 @@ struct Request {
     std::vector<double *> pin;
     std::vector<std::unique_ptr<double[]>> src;
     std::vector<double *> sol;  // pinned, same layout, filled on completion
-    const double *source(int k) const { return pin[k] ? pin[k] : src[k].get(); }
+    int mode = REQ_HOST_LEX;
+    // REQ_HOST_EO: the caller's page-locked sources (read by DMA; null: staged in pin) and
+    // solution arrays (written by DMA when page-locked, else copied from sol at wait)
+    std::vector<const double *> src_direct;
+    std::vector<double *> user_sol;
+    std::vector<char> sol_direct;
+    // REQ_FIELDS: EVEN halves of the caller's device fields
+    std::vector<double2 *> fb, fx;
+    uint64_t admit_chunk = 0, retire_chunk = 0;  // server chunks launched before admission / retirement
+    const double *source(int k) const {
+        if (!src_direct.empty() && src_direct[k]) return src_direct[k];
+        return pin[k] ? pin[k] : src[k].get();
+    }
     std::vector<int> slots;
     size_t bytes = 0;
     ReqState state = REQ_QUEUED;
@@ -236,8 +265,17 @@ int admit_waiting(hw_server *S) {
         S->bytes_in_use += need;
         q->t_admit = Clock::now();
         const int stride = E.lattice(l).stride;
+        q->admit_chunk = S->stats.chunks;
         for (int k = 0; k < q->nrhs; k++) {
             int slot;
+            if (q->mode == REQ_FIELDS) {
+                // the engine reads b and accumulates x in the caller's fields (x: initial guess)
+                if ((rc = E.admit(l, q->kappa, q->fb[k], q->fx[k], q->tol, q->maxiters, S->cfg.delta,
+                                  ENG_MODE_SOLVE, &slot)) != HW_OK)
+                    return rc;
+                q->slots.push_back(slot);
+                continue;
+            }
             if ((rc = E.admit(l, q->kappa, nullptr, nullptr, q->tol, q->maxiters, S->cfg.delta, ENG_MODE_SOLVE,
                               &slot)) != HW_OK)
                 return rc;
@@ -311,24 +349,34 @@ int retire_finished(hw_server *S) {
                     status = HW_ERR_BREAKDOWN;
                 else if (s.status != ENG_CONVERGED && status == HW_OK)
                     status = HW_ERR_NOT_CONVERGED;
-                // the pinned source buffer (its copy to the device finished earlier on this
-                // stream) receives the solution
-                q->sol[k] = q->pin[k] ? q->pin[k] : S->pool.get(q->n);
-                q->pin[k] = nullptr;
-                if (!q->sol[k]) {
-                    set_error("page-locked host allocation of %zu bytes failed", q->n * sizeof(double));
-                    return HW_ERR_OOM;
+                if (q->mode == REQ_FIELDS) continue;  // the solution is in the caller's field
+                // the caller's page-locked solution array, or the pinned source buffer (its
+                // copy to the device finished earlier on this stream), receives the solution
+                double *dst;
+                if (q->mode == REQ_HOST_EO && q->sol_direct[k]) {
+                    dst = q->user_sol[k];
+                } else {
+                    q->sol[k] = q->pin[k] ? q->pin[k] : S->pool.get(q->n);
+                    q->pin[k] = nullptr;
+                    if (!q->sol[k]) {
+                        set_error("page-locked host allocation of %zu bytes failed", q->n * sizeof(double));
+                        return HW_ERR_OOM;
+                    }
+                    dst = q->sol[k];
                 }
                 const int l = E.slot_lattice(slot);
                 double *stage = reinterpret_cast<double *>(E.own_b(slot));
                 launch_soa_to_aos((int)G.Vh, HalfF64{E.own_x(slot), E.lattice(l).stride}, stage, S->copy_stream);
                 S->layout_launches++;
-                HW_CUDA(cudaMemcpyAsync(q->sol[k], stage, q->n * sizeof(double), cudaMemcpyDeviceToHost,
+                HW_CUDA(cudaMemcpyAsync(dst, stage, q->n * sizeof(double), cudaMemcpyDeviceToHost,
                                         S->copy_stream));
             }
             S->stats.completed++;
             S->stats.solves_completed += q->nrhs;
         }
+        q->retire_chunk = S->stats.chunks;
+        q->res.admit_chunk = q->admit_chunk;
+        q->res.retire_chunk = q->retire_chunk;
         // a slot's buffers are reused only by copy-stream work queued after these copies
         for (int slot : q->slots) E.release(slot);
         S->bytes_in_use -= q->bytes;
@@ -518,33 +566,76 @@ int hw_server_add_gauge(hw_server *S, const hw_gauge *gauge, int *gauge_id) {
     return HW_OK;
 }
 
-int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const double *const *sources,
-                     double accuracy, int maxiters, uint64_t *request_id) {
-    HW_CHECK_ARG(S && sources && request_id, "null argument");
+}  // extern "C"
+
+namespace hw {
+namespace {
+
+// checks shared by every submit form; G receives the gauge's lattice
+int submit_check(hw_server *S, int gauge_id, int nrhs, double accuracy, int maxiters, GaugeEntry *G) {
     HW_CHECK_ARG(nrhs >= 1 && nrhs <= kEngMaxRhs, "nrhs must be 1..%d", kEngMaxRhs);
     HW_CHECK_ARG(accuracy > 0 && maxiters > 0, "bad accuracy or maxiters");
-    for (int k = 0; k < nrhs; k++) HW_CHECK_ARG(sources[k], "source %d is null", k);
-    GaugeEntry G;
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
-        HW_CHECK_ARG(gauge_id >= 0 && gauge_id < (int)S->gauges.size(), "unknown gauge id %d", gauge_id);
-        if (!S->worker_error.empty()) {
-            set_error("server failed: %s", S->worker_error.c_str());
-            return HW_ERR_CUDA;
-        }
-        G = S->gauges[gauge_id];
+    std::lock_guard<std::mutex> lk(S->mu);
+    HW_CHECK_ARG(gauge_id >= 0 && gauge_id < (int)S->gauges.size(), "unknown gauge id %d", gauge_id);
+    if (!S->worker_error.empty()) {
+        set_error("server failed: %s", S->worker_error.c_str());
+        return HW_ERR_CUDA;
     }
+    *G = S->gauges[gauge_id];
+    return HW_OK;
+}
+
+std::shared_ptr<Request> new_request(hw_server *S, const GaugeEntry &G, int gauge_id, double kappa, int nrhs,
+                                      double accuracy, int maxiters, int mode) {
     std::shared_ptr<Request> q(new Request());
     q->gauge_id = gauge_id;
     q->kappa = kappa;
     q->tol = accuracy;
     q->maxiters = maxiters;
     q->nrhs = nrhs;
+    q->mode = mode;
     q->t_submit = Clock::now();
     q->pool = &S->pool;
     q->n = (size_t)G.Vh * 24;
     q->pin.assign(nrhs, nullptr);
     q->src.resize(nrhs);
+    return q;
+}
+
+// queue a request (or reject one that can never fit the memory budget)
+int enqueue_request(hw_server *S, const GaugeEntry &G, std::shared_ptr<Request> q, uint64_t *request_id) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    q->id = S->next_id++;
+    S->stats.submitted++;
+    S->all[q->id] = q;
+    *request_id = q->id;
+    const size_t need = (size_t)q->nrhs * S->eng->slot_bytes_for_stride(padded_stride(G.Vh));
+    if (need > S->cfg.hbm_budget_bytes) {
+        q->release_sources();
+        q->state = REQ_DONE;
+        q->res.status = HW_ERR_REJECTED;
+        q->res.nrhs = q->nrhs;
+        S->stats.rejected++;
+        return HW_OK;
+    }
+    S->queue.push_back(q);
+    S->cv_work.notify_all();
+    return HW_OK;
+}
+
+}  // namespace
+}  // namespace hw
+
+extern "C" {
+
+int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const double *const *sources,
+                     double accuracy, int maxiters, uint64_t *request_id) {
+    HW_CHECK_ARG(S && sources && request_id, "null argument");
+    GaugeEntry G;
+    int rc = submit_check(S, gauge_id, nrhs, accuracy, maxiters, &G);
+    if (rc != HW_OK) return rc;
+    for (int k = 0; k < nrhs; k++) HW_CHECK_ARG(sources[k], "source %d is null", k);
+    std::shared_ptr<Request> q = new_request(S, G, gauge_id, kappa, nrhs, accuracy, maxiters, REQ_HOST_LEX);
     for (int k = 0; k < nrhs; k++) {
         double *dst = q->pin[k] = S->pool.get(q->n);
         if (!dst) {
@@ -553,24 +644,53 @@ int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const d
         }
         gather_even(G, sources[k], dst);
     }
-    std::lock_guard<std::mutex> lk(S->mu);
-    q->id = S->next_id++;
-    S->stats.submitted++;
-    S->all[q->id] = q;
-    *request_id = q->id;
-    // a request that can never fit the budget is rejected now
-    const size_t need = (size_t)nrhs * S->eng->slot_bytes_for_stride(padded_stride(G.Vh));
-    if (need > S->cfg.hbm_budget_bytes) {
-        q->release_sources();
-        q->state = REQ_DONE;
-        q->res.status = HW_ERR_REJECTED;
-        q->res.nrhs = nrhs;
-        S->stats.rejected++;
-        return HW_OK;
+    return enqueue_request(S, G, q, request_id);
+}
+
+int hw_server_submit_eo(hw_server *S, int gauge_id, double kappa, int nrhs, const double *const *sources,
+                        double *const *solutions, double accuracy, int maxiters, uint64_t *request_id) {
+    HW_CHECK_ARG(S && sources && solutions && request_id, "null argument");
+    GaugeEntry G;
+    int rc = submit_check(S, gauge_id, nrhs, accuracy, maxiters, &G);
+    if (rc != HW_OK) return rc;
+    for (int k = 0; k < nrhs; k++) HW_CHECK_ARG(sources[k] && solutions[k], "source or solution %d is null", k);
+    std::shared_ptr<Request> q = new_request(S, G, gauge_id, kappa, nrhs, accuracy, maxiters, REQ_HOST_EO);
+    q->src_direct.assign(nrhs, nullptr);
+    q->user_sol.assign(solutions, solutions + nrhs);
+    q->sol_direct.assign(nrhs, 0);
+    for (int k = 0; k < nrhs; k++) {
+        q->sol_direct[k] = host_pinned(solutions[k]) ? 1 : 0;
+        if (host_pinned(sources[k])) {
+            q->src_direct[k] = sources[k];  // read by DMA at admission
+            continue;
+        }
+        // pageable: one contiguous copy of the EVEN half into a page-locked buffer
+        double *dst = q->pin[k] = S->pool.get(q->n);
+        if (!dst) {
+            q->src[k].reset(new double[q->n]);
+            dst = q->src[k].get();
+        }
+        std::memcpy(dst, sources[k], q->n * sizeof(double));
     }
-    S->queue.push_back(q);
-    S->cv_work.notify_all();
-    return HW_OK;
+    return enqueue_request(S, G, q, request_id);
+}
+
+int hw_server_submit_fields(hw_server *S, int gauge_id, double kappa, int nrhs, const hw_field *const *sources,
+                            hw_field *const *solutions, double accuracy, int maxiters, uint64_t *request_id) {
+    HW_CHECK_ARG(S && sources && solutions && request_id, "null argument");
+    GaugeEntry G;
+    int rc = submit_check(S, gauge_id, nrhs, accuracy, maxiters, &G);
+    if (rc != HW_OK) return rc;
+    std::shared_ptr<Request> q = new_request(S, G, gauge_id, kappa, nrhs, accuracy, maxiters, REQ_FIELDS);
+    for (int k = 0; k < nrhs; k++) {
+        HW_CHECK_ARG(sources[k] && solutions[k], "source or solution field %d is null", k);
+        HW_CHECK_ARG(sources[k]->lat == G.gauge->lat && solutions[k]->lat == G.gauge->lat,
+                     "field %d belongs to another lattice than the gauge field", k);
+        HW_CHECK_ARG(sources[k] != solutions[k], "source and solution %d are the same field", k);
+        q->fb.push_back(const_cast<double2 *>(sources[k]->half[0].buf.as<double2>()));
+        q->fx.push_back(solutions[k]->half[0].buf.as<double2>());
+    }
+    return enqueue_request(S, G, q, request_id);
 }
 
 int hw_server_wait(hw_server *S, uint64_t request_id, double *const *solutions, double timeout_seconds,
@@ -591,9 +711,14 @@ int hw_server_wait(hw_server *S, uint64_t request_id, double *const *solutions, 
     S->all.erase(request_id);
     const GaugeEntry G = S->gauges[q->gauge_id];
     lk.unlock();
-    if (solutions && !q->sol.empty())
+    if (q->mode == REQ_HOST_EO && !q->sol.empty()) {
+        // solutions that could not be written by DMA (pageable arrays): the EVEN half
+        for (int k = 0; k < q->nrhs; k++)
+            if (!q->sol_direct[k] && q->sol[k]) std::memcpy(q->user_sol[k], q->sol[k], q->n * sizeof(double));
+    } else if (q->mode == REQ_HOST_LEX && solutions && !q->sol.empty()) {
         for (int k = 0; k < q->nrhs; k++)
             if (solutions[k]) scatter_even(G, q->sol[k], solutions[k]);
+    }
     return q->res.status == HW_ERR_CANCELLED || q->res.status == HW_ERR_REJECTED ? q->res.status : HW_OK;
 }
 

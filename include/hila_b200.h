@@ -120,6 +120,13 @@ int hw_field_destroy(hw_field *field);
 /* copy sites of `parity` from/to a host array in the canonical layout */
 int hw_field_upload(hw_field *field, const double *host, int parity);
 int hw_field_download(const hw_field *field, double *host, int parity);
+/* the same with the host array in HILA's even-first site order (its Field storage
+ * order, lattice.cpp:171-184: the V/2 EVEN sites, then the V/2 ODD sites, each
+ * double[4][3][2]): a parity is one contiguous block, so only the sites of `parity`
+ * cross the bus (one copy per parity, at full rate from page-locked memory) and the
+ * other parity of the host array is left as it is */
+int hw_field_upload_eo(hw_field *field, const double *host, int parity);
+int hw_field_download_eo(const hw_field *field, double *host, int parity);
 /* field[parity] = 0 */
 int hw_field_zero(hw_field *field, int parity);
 
@@ -286,6 +293,9 @@ typedef struct hw_request_result {
     double true_residual;     /* largest |b - M x| / |b| over the sources (FP64) */
     double latency_seconds;   /* submit -> result available */
     double queue_seconds;     /* submit -> admitted */
+    uint64_t admit_chunk;     /* chunks the server had launched when the request was admitted ... */
+    uint64_t retire_chunk;    /* ... and when it retired: a request admitted while another one's
+                                 [admit_chunk, retire_chunk) interval was open ran beside it */
 } hw_request_result;
 
 typedef struct hw_server_stats {
@@ -308,10 +318,28 @@ int hw_server_add_gauge(hw_server *server, const hw_gauge *gauge, int *gauge_id)
  * the sources are copied before the call returns */
 int hw_server_submit(hw_server *server, int gauge_id, double kappa, int nrhs, const double *const *sources,
                      double accuracy, int maxiters, uint64_t *request_id);
+/* queue M x = b for nrhs host sources in HILA's even-first site order (the order of
+ * its Field storage, lattice.cpp:171-184: the V/2 EVEN sites first, each site
+ * double[4][3][2]); only the EVEN half of each source is read and only the EVEN half
+ * of each solution written.  Page-locked arrays (cudaHostAlloc / cudaHostRegister)
+ * are read and written by DMA directly: the caller keeps them valid and unread until
+ * the request's wait returns.  Pageable sources are copied before the call returns;
+ * pageable solutions are filled by hw_server_wait. */
+int hw_server_submit_eo(hw_server *server, int gauge_id, double kappa, int nrhs, const double *const *sources,
+                        double *const *solutions, double accuracy, int maxiters, uint64_t *request_id);
+/* queue M x = b for nrhs device fields of the gauge field's lattice (the form HILA's
+ * fermion code holds, hmc/fermion_field.h:90-103): the engine reads the EVEN half of
+ * sources[k] and accumulates the solution in the EVEN half of solutions[k], whose
+ * content on submit is the initial guess (zero it for none).  Nothing is copied; the
+ * caller leaves the fields alone until the request's wait returns. */
+int hw_server_submit_fields(hw_server *server, int gauge_id, double kappa, int nrhs, const hw_field *const *sources,
+                            hw_field *const *solutions, double accuracy, int maxiters, uint64_t *request_id);
 /* wait up to timeout_seconds (< 0: forever) for a request; on completion copy
- * its solutions (canonical layout, ODD sites zero) into solutions[0..nrhs-1]
- * (solutions or an entry may be NULL) and fill *result.  HW_ERR_TIMEOUT if
- * still running.  A finished request is forgotten after its wait. */
+ * the solutions of an hw_server_submit request (canonical layout, ODD sites zero)
+ * into solutions[0..nrhs-1] (solutions or an entry may be NULL; requests of the
+ * other submit forms have their solutions in place and ignore it) and fill
+ * *result.  HW_ERR_TIMEOUT if still running.  A finished request is forgotten
+ * after its wait. */
 int hw_server_wait(hw_server *server, uint64_t request_id, double *const *solutions, double timeout_seconds,
                    hw_request_result *result);
 /* cancel a queued or running request (its slots are freed at the next chunk) */
