@@ -75,7 +75,7 @@ class _CgResult(ctypes.Structure):
 
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("delta", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_size_t),
-                ("chunk_iters", ctypes.c_int)]
+                ("chunk_iters", ctypes.c_int), ("host_pool_bytes", ctypes.c_size_t)]
 
 
 class _RequestResult(ctypes.Structure):
@@ -104,6 +104,12 @@ class _SolveRequest(ctypes.Structure):
     _fields_ = [("gauge", ctypes.c_void_p), ("kappa", ctypes.c_double), ("b", ctypes.c_void_p),
                 ("x", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int),
                 ("hasenbusch_mh", ctypes.c_double)]
+
+
+class _StagSolveRequest(ctypes.Structure):
+    _fields_ = [("gauge", ctypes.c_void_p), ("mass", ctypes.c_double), ("inp", ctypes.c_void_p),
+                ("out", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int),
+                ("normal", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p
@@ -148,10 +154,15 @@ _SIGNATURES = {
     "hw_staggered_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_staggered_evenodd_force": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, _dp]),
     "hw_staggered_cg_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, _vp, _vp]),
+    "hw_staggered_batch_solve": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp]),
+    "hw_server_submit_staggered": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_double,
+                                                  ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "hw_gauge_config_dims": (ctypes.c_int, [ctypes.c_char_p, _ip]),
     "hw_gauge_config_write": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
     "hw_gauge_config_read": (ctypes.c_int, [ctypes.c_char_p, _ip, _dp]),
     "hw_wilson_apply": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    "hw_wilson_cg_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, _vp, _vp]),
     "hw_wilson_hop": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "hw_cg_params_default": (None, [ctypes.POINTER(_CgParams)]),
     "hw_cg_solve": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.POINTER(_CgParams),
@@ -432,9 +443,10 @@ class Field:
 
     def upload_eo(self, data: np.ndarray, parity: int = ALL):
         """hw_field_upload_eo: `data` in even-first site order ((V,4,3,2), EVEN sites first);
-        only the sites of `parity` are copied."""
-        if data.dtype != np.float64 or not data.flags.c_contiguous or data.size != self.lattice.volume * 24:
-            raise ValueError("spinor arrays hold V*24 contiguous doubles")
+        only the sites of `parity` are copied (for EVEN a (V/2,4,3,2) array suffices)."""
+        need = self.lattice.volume * (12 if parity == EVEN else 24)
+        if data.dtype != np.float64 or not data.flags.c_contiguous or data.size < need:
+            raise ValueError("spinor arrays hold V*24 contiguous doubles (V*12 for the EVEN half)")
         _check(lib().hw_field_upload_eo(self.handle, _dptr(data), int(parity)))
 
     def download_eo(self, parity: int = ALL, out: np.ndarray | None = None) -> np.ndarray:
@@ -442,8 +454,9 @@ class Field:
         other parity of `out` is left as it is."""
         if out is None:
             out = np.zeros((self.lattice.volume, 4, 3, 2), np.float64)
-        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.lattice.volume * 24:
-            raise ValueError("spinor arrays hold V*24 contiguous doubles")
+        need = self.lattice.volume * (12 if parity == EVEN else 24)
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size < need:
+            raise ValueError("spinor arrays hold V*24 contiguous doubles (V*12 for the EVEN half)")
         _check(lib().hw_field_download_eo(self.handle, _dptr(out), int(parity)))
         return out
 
@@ -636,6 +649,17 @@ class Dirac_Wilson:
     def dagger(self, inp: Field, out: Field):
         _check(lib().hw_wilson_apply(self.gauge.handle, self.kappa, -1, inp.handle, out.handle))
 
+    def cg(self, inp: Field, out: Field, accuracy: float = 1e-12, maxiters: int = 10000,
+           true_residual: bool = False) -> "CGResult":
+        """CG<Dirac_Wilson>::apply (hw_wilson_cg_solve): M^dag M out = inp on ALL sites, FP64."""
+        p = _params(accuracy, maxiters, "f64", 0.1, true_residual, False)
+        r = _CgResult()
+        rc = lib().hw_wilson_cg_solve(self.gauge.handle, self.kappa, inp.handle, out.handle, ctypes.byref(p),
+                                      ctypes.byref(r))
+        if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+            _check(rc)
+        return CGResult.from_c(r)
+
 
 @dataclass
 class CGResult:
@@ -726,6 +750,26 @@ def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0
     return [CGResult.from_c(res[k]) for k in range(n)]
 
 
+def staggered_batch_solve(ctx: Context, requests) -> list:
+    """Many staggered solves at once on the batched engine (hw_staggered_batch_solve):
+    requests are (dirac_staggered_evenodd, in_field, out_field[, accuracy[, maxiters[, normal]]]);
+    normal=False solves M out = in, normal=True M^dag M out = in (CG<Op>::apply)."""
+    n = len(requests)
+    arr = (_StagSolveRequest * max(n, 1))()
+    for k, req in enumerate(requests):
+        op, b, x = req[0], req[1], req[2]
+        acc = req[3] if len(req) > 3 else 1e-10
+        mi = req[4] if len(req) > 4 else 10000
+        normal = req[5] if len(req) > 5 else False
+        arr[k] = _StagSolveRequest(op.gauge.handle.value, op.mass, b.handle.value, x.handle.value, float(acc),
+                                   int(mi), int(bool(normal)))
+    res = (_CgResult * max(n, 1))()
+    rc = lib().hw_staggered_batch_solve(ctx.handle, arr, n, res)
+    if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):
+        _check(rc)
+    return [CGResult.from_c(res[k]) for k in range(n)]
+
+
 def wilson_evenodd_apply_noalloc(dims, kappa: float, sign: int, links_ptr: int, in_ptr: int, out_ptr: int,
                                  stride: int, link_format: int = 18, antiperiodic: bool = True,
                                  stream: int = 0) -> None:
@@ -791,8 +835,9 @@ class Server:
     bitwise the same alone and in any mix."""
 
     def __init__(self, ctx: Context, precision: str = "f16", delta: float = 0.0, hbm_budget_bytes: int = 0,
-                 chunk_iters: int = 8):
-        cfg = _ServerConfig(PRECISIONS[precision], float(delta), int(hbm_budget_bytes), int(chunk_iters))
+                 chunk_iters: int = 8, host_pool_bytes: int = 0):
+        cfg = _ServerConfig(PRECISIONS[precision], float(delta), int(hbm_budget_bytes), int(chunk_iters),
+                            int(host_pool_bytes))
         self.ctx = ctx
         self.handle = _vp()
         _check(lib().hw_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(self.handle)))
@@ -813,13 +858,15 @@ class Server:
 
     def submit_eo(self, gauge_id: int, kappa: float, sources, solutions, accuracy: float = 1e-10,
                   maxiters: int = 10000) -> int:
-        """hw_server_submit_eo: host arrays in even-first site order ((V,4,3,2), EVEN sites first).
-        Page-locked arrays (PinnedArray) are copied by DMA directly; keep every array alive and
-        untouched until wait() returns, which also fills pageable solutions."""
-        for a in list(sources) + list(solutions):
+        """hw_server_submit_eo: host arrays in even-first site order ((V,4,3,2), EVEN sites first;
+        only the EVEN half is used, so (V/2,4,3,2) arrays suffice).  Page-locked arrays
+        (PinnedArray) are copied by DMA directly; keep every array alive and untouched until
+        wait() returns, which also fills pageable solutions.  solutions=None: the solutions
+        stay in the server's buffers (wait(copy=True) returns them in even-first order)."""
+        for a in list(sources) + list(solutions or []):
             assert a.dtype == np.float64 and a.flags.c_contiguous
         src = (_dp * len(sources))(*[_dptr(a) for a in sources])
-        sol = (_dp * len(solutions))(*[_dptr(a) for a in solutions])
+        sol = (_dp * len(solutions))(*[_dptr(a) for a in solutions]) if solutions else None
         rid = ctypes.c_uint64()
         _check(lib().hw_server_submit_eo(self.handle, int(gauge_id), float(kappa), len(sources), src, sol,
                                          float(accuracy), int(maxiters), ctypes.byref(rid)))
@@ -835,6 +882,16 @@ class Server:
                                              float(accuracy), int(maxiters), ctypes.byref(rid)))
         return rid.value
 
+    def submit_staggered(self, gauge_id: int, mass: float, sources, solutions, accuracy: float = 1e-10,
+                         maxiters: int = 10000) -> int:
+        """hw_server_submit_staggered: staggered M x = b on device StaggeredFields, in place."""
+        src = (_vp * len(sources))(*[f.handle for f in sources])
+        sol = (_vp * len(solutions))(*[f.handle for f in solutions])
+        rid = ctypes.c_uint64()
+        _check(lib().hw_server_submit_staggered(self.handle, int(gauge_id), float(mass), len(sources), src, sol,
+                                                float(accuracy), int(maxiters), ctypes.byref(rid)))
+        return rid.value
+
     def wait(self, request_id: int, nrhs: int, volume: int, timeout: float = -1.0, copy: bool = True):
         """Returns (solutions, RequestResult); solutions is a list of (V,4,3,2)
         arrays, or None with copy=False."""
@@ -848,6 +905,15 @@ class Server:
             _check(rc)
         return sols, RequestResult(r.status, r.nrhs, r.iterations, r.reliable_updates, r.true_residual,
                                    r.latency_seconds, r.queue_seconds, r.admit_chunk, r.retire_chunk)
+
+    def poll(self, request_id: int, nrhs: int, volume: int, copy: bool = False):
+        """wait() that returns None at once while the request is still running."""
+        try:
+            return self.wait(request_id, nrhs, volume, timeout=0.0, copy=copy)
+        except HilaError as e:
+            if e.code == HW_ERR_TIMEOUT:
+                return None
+            raise
 
     def cancel(self, request_id: int) -> None:
         _check(lib().hw_server_cancel(self.handle, ctypes.c_uint64(request_id)))

@@ -112,19 +112,22 @@ int Engine::ensure_partials() {
     return HW_OK;
 }
 
-int Engine::lattice_index(const hw_gauge *G, int *idx) {
+int Engine::lattice_index(const hw_gauge *G, int *idx, int fermion) {
+    HW_CHECK_ARG(fermion == FERM_WILSON || fermion == FERM_STAGGERED, "unknown fermion kind %d", fermion);
     for (int l = 0; l < tables_.nlat; l++)
-        if (gauges_[l] == G) {
+        if (gauges_[l] == G && tables_.lat[l].fermion == fermion) {
             *idx = l;
             return HW_OK;
         }
     HW_CHECK_ARG(tables_.nlat < kEngMaxLat, "engine holds %d lattices already", kEngMaxLat);
     int rc;
-    if ((rc = ensure_low_links(G, low_, full18_)) != HW_OK) return rc;
+    // staggered solves run in FP64 and need no low-precision links
+    if (fermion == FERM_WILSON && (rc = ensure_low_links(G, low_, full18_)) != HW_OK) return rc;
     hw_lattice *lat = G->lat;
     const int l = tables_.nlat;
     EngLattice &L = tables_.lat[l];
     std::memset(&L, 0, sizeof(L));
+    L.fermion = fermion;
     L.g = lat->g;
     L.stride = lat->stride;
     L.ntiles = (int)((lat->Vh + kEngTile - 1) / kEngTile);
@@ -199,8 +202,8 @@ int Engine::free_slots_on(int lat) const {
 size_t Engine::slot_bytes_for_stride(int stride) const {
     const size_t st = stride;
     const size_t low_site = low_ == LOW_F16 ? (48 + 4) : 96;
-    // p, r, Dp, t (low) + y (FP32) + s, t64 (FP64) + owned x, b (FP64)
-    return st * (4 * low_site + 96 + 2 * 192) + st * 2 * 192;
+    // p, r, Dp, t (low) + y (FP32) + s, t64 (FP64) + owned x, b and solution staging (FP64)
+    return st * (4 * low_site + 96 + 2 * 192) + st * 3 * 192;
 }
 
 size_t Engine::slot_bytes(int lat) const { return slot_bytes_for_stride(tables_.lat[lat].stride); }
@@ -210,7 +213,7 @@ int Engine::ensure_slot_buffers(int slot, int stride) {
     if (B.stride >= stride && B.p.ptr) return HW_OK;
     const size_t st = stride;
     int rc;
-    for (DevBuf *d : {&B.x_own, &B.b_own}) d->release();
+    for (DevBuf *d : {&B.x_own, &B.b_own, &B.xfer}) d->release();
     if (low_ == LOW_F16) {
         for (DevBuf *d : {&B.p, &B.r, &B.Dp, &B.t})
             if ((rc = d->alloc(3 * st * sizeof(uint4))) != HW_OK) return rc;
@@ -236,6 +239,8 @@ int Engine::ensure_own(int slot) {
         if ((rc = B.x_own.alloc(bytes)) != HW_OK) return rc;
     if (!B.b_own.ptr || B.b_own.bytes < bytes)
         if ((rc = B.b_own.alloc(bytes)) != HW_OK) return rc;
+    if (!B.xfer.ptr || B.xfer.bytes < bytes)
+        if ((rc = B.xfer.alloc(bytes)) != HW_OK) return rc;
     return HW_OK;
 }
 
@@ -287,6 +292,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     std::memset(&S, 0, sizeof(S));
     S.status = ENG_RUNNING;
     S.mode = mode;
+    S.fermion = L.fermion;
     S.ru = 1;
     S.init = 1;
     S.tol2 = tol * tol;
@@ -374,9 +380,13 @@ int Engine::build_graph() {
 }
 
 int Engine::configure() {
-    int mask = 0;
-    for (int l = 0; l < tables_.nlat; l++) mask |= tables_.lat[l].l64_planes == 9 ? 1 : 2;
+    int mask = 0, fermions = 0;
+    for (int l = 0; l < tables_.nlat; l++) {
+        mask |= tables_.lat[l].l64_planes == 9 ? 1 : 2;
+        fermions |= 1 << tables_.lat[l].fermion;
+    }
     if (mask == 0) mask = 1;
+    if (fermions == 0) fermions = 1;
     int variant = default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
     // launch shapes (engine.cu): 2 for both precisions, 4 and 7 for FP16 only; the
@@ -384,8 +394,9 @@ int Engine::configure() {
     const bool known =
         variant == 2 || (low_ == LOW_F16 && (variant == 7 || (variant == 4 && full18_)));
     if (!known) variant = default_variant();
-    if (variant != grid_.variant || mask != grid_.planes_mask) {
+    if (variant != grid_.variant || mask != grid_.planes_mask || fermions != grid_.fermions) {
         grid_ = eng_grid_size(low_, variant, full18_ ? 1 : 0, mask);
+        grid_.fermions = fermions;  // the phases the iteration launches (engine.cu)
         if (chunk_exec_) {
             HW_CUDA(cudaStreamSynchronize(ctx_->stream));
             cudaGraphExecDestroy(chunk_exec_);

@@ -14,6 +14,7 @@
 #include "engine.h"
 #include "pair.cuh"
 #include "reduce.cuh"
+#include "staggered_math.cuh"
 #include "storage.cuh"
 
 namespace hw {
@@ -71,8 +72,9 @@ __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
 
 // Which slots take part in a phase.  States only change in the finishers,
 // which run after every tile of the lattice is done, so all blocks agree.
-template <int PHASE>
+template <int PHASE, int FERM = FERM_WILSON>
 __device__ __forceinline__ bool active(const EngState &s) {
+    if (s.fermion != FERM) return false;  // the other fermion's kernels serve this slot
     // the first update of a solve from x = 0: H x is zero, R2 has nothing to do
     if (PHASE == PH_R2) return s.ru != 0 && !(s.init && !s.xnz);
     if (PHASE == PH_R4 || PHASE == PH_R5) return s.ru != 0 && s.mode == ENG_MODE_NORMAL;
@@ -106,7 +108,7 @@ struct ActiveTable {
     int n[kEngMaxLat];
 };
 
-template <int PHASE>
+template <int PHASE, int FERM = FERM_WILSON>
 __device__ __forceinline__ void build_active(const EngPtrs &P, ActiveTable &A) {
     const EngTables *T = P.T;
     for (int l = threadIdx.x; l < T->nlat; l += blockDim.x) {
@@ -114,7 +116,7 @@ __device__ __forceinline__ void build_active(const EngPtrs &P, ActiveTable &A) {
         int na = 0;
         for (int q = 0; q < La.nprob; q++) {
             const int j = La.prob[q];
-            if (active<PHASE>(P.S[j])) A.slot[l][na++] = j;
+            if (active<PHASE, FERM>(P.S[j])) A.slot[l][na++] = j;
         }
         A.n[l] = na;
     }
@@ -332,7 +334,7 @@ __device__ void finish(EngState &s, const EngProblem &pr, const double *tot, int
 // Arrival of one work item of lattice l (a tile, or a (tile, slot) pair: the
 // lattice expects `expected` of them); the last arrival sums every active
 // slot's partials in tile order and runs the finisher.
-template <int PHASE, int NRED>
+template <int PHASE, int NRED, int FERM = FERM_WILSON>
 __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLattice &La, int l, double *smem,
                                                   bool &last, int expected) {
     const EngTables *T = P.T;
@@ -348,7 +350,7 @@ __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLat
         const int max_tiles = T->max_tiles;
         for (int q = 0; q < La.nprob; q++) {
             const int j = La.prob[q];
-            if (!active<PHASE>(P.S[j])) continue;
+            if (!active<PHASE, FERM>(P.S[j])) continue;
             double tot[2] = {0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < NRED; k++) {
@@ -366,6 +368,7 @@ __device__ __forceinline__ void arrive_and_finish(const EngPtrs &P, const EngLat
 }
 
 #include "engine_mma.cuh"
+#include "engine_stag.cuh"
 
 // Inner phases P1..P4 in low precision.  Each thread owns one site and up to
 // NR right-hand sides at a time, so links, their third rows and the neighbour
@@ -861,10 +864,14 @@ void enqueue_iteration_nr(const EngPtrs &P, const EngGrid &G, cudaStream_t s, co
 }  // namespace
 
 void eng_enqueue_iteration(int low, const EngPtrs &P, const EngGrid &G, cudaStream_t s, const cudaEvent_t *ev) {
-    if (low == LOW_F16)
-        enqueue_iteration_nr<LOW_F16>(P, G, s, ev);
-    else
-        enqueue_iteration_nr<LOW_F32>(P, G, s, ev);
+    if (G.fermions & 1) {
+        if (low == LOW_F16)
+            enqueue_iteration_nr<LOW_F16>(P, G, s, ev);
+        else
+            enqueue_iteration_nr<LOW_F32>(P, G, s, ev);
+    }
+    // staggered phases after the Wilson ones (outside the profiling events)
+    if (G.fermions & 2) enqueue_stag_iteration(P, G, s);
 }
 
 void eng_enqueue_control(const EngPtrs &P, int nprob, int chunk, cudaGraphConditionalHandle h, int use_cond,
@@ -908,6 +915,7 @@ EngGrid eng_grid_size(int low, int variant, int full18, int planes_mask) {
     G.pk = G.low;
     if (variant == 7 && low == LOW_F16) G.pk = sms * occupancy_low<LOW_F16, 2, 3, true, PH_P1>();
     G.f64 = sms * (hi < 1 ? 1 : hi);
+    G.fermions = 1;
     G.variant = variant;
     G.full18 = full18;
     G.planes_mask = planes_mask;

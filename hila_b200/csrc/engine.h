@@ -38,6 +38,13 @@ constexpr int kEngMaxProb = 64;    // solve slots per engine
 constexpr int kEngMaxRhs = 16;     // slots per lattice
 
 enum EngStatus : int { ENG_RUNNING = 0, ENG_CONVERGED = 1, ENG_MAXITER = 2, ENG_BREAKDOWN = 3, ENG_IDLE = 4 };
+// fermion of a lattice entry (and of its slots).  Staggered solves (staggered.h) run the
+// same phase sequence and state machine in FP64 on colour-vector fields (engine_stag.cuh):
+//   P1 t = (1/m) D^{oe}_+ p   P2 Dp = m p + D^{eo}_+ t, |Dp|^2   P3 t = (1/m) D^{oe}_- Dp
+//   P4 r -= alpha (m Dp + D^{eo}_- t), x += alpha p (FP64), |r|^2
+//   R1 flags a nonzero initial x; R2, R3 s = b - M x; R4(L), R5(L) r = M^dag s; P5 p = r + beta p
+// with D_s = 0.5 s hop (staggered.h:48-68) and the slot's kappa holding the mass m.
+enum EngFermion : int { FERM_WILSON = 0, FERM_STAGGERED = 1 };
 enum EngMode : int { ENG_MODE_SOLVE = 0, ENG_MODE_NORMAL = 1 };
 
 struct EngLattice {
@@ -46,6 +53,7 @@ struct EngLattice {
     int tile0;        // first global tile
     int ntiles;       // tiles of one parity
     int nprob;        // slots on this lattice
+    int fermion;      // EngFermion of the lattice entry (one gauge field may have one of each)
     int prob[kEngMaxRhs];
     // links: FP64 (18 or 12 reals) for the reliable updates, low precision for the inner solve
     const double2 *l64;
@@ -91,6 +99,7 @@ struct EngState {
     int n_ru;
     int mode;        // EngMode of the slot (copy of its problem's, read by the phase selection)
     int xnz;         // 1: the initial x has a nonzero component (set by R1 of the first update)
+    int fermion;     // EngFermion of the slot's lattice (read by the phase selection)
 };
 
 struct EngTables {
@@ -131,6 +140,7 @@ struct EngGrid {
     int variant;  // launch shape of the low-precision phases (engine.cu)
     int full18;   // 1: inner phases read 18-real links (FP32 or FP16); 0: the 12-real links of the precision
     int planes_mask;  // FP64 link formats present: bit 0 = 18 reals, bit 1 = 12 reals
+    int fermions;     // lattice kinds present: bit 0 Wilson, bit 1 staggered (phases launched)
 };
 
 // in launch order; R4 / R5 serve slots of the normal system (FP64), R4L / R5L those of

@@ -12,6 +12,7 @@ namespace hw {
 struct SlotBuffers {
     DevBuf p, r, Dp, t, pn, rn, Dpn, tn, y, s, t64;
     DevBuf x_own, b_own;  // FP64 EVEN halves for slots that own their source / solution
+    DevBuf xfer;          // layout staging of an owned solution on its way to the host
     int stride = 0;
 };
 
@@ -28,8 +29,9 @@ class Engine {
     int low() const { return low_; }
     bool full18() const { return full18_; }  // inner phases read 18-real links
 
-    // index of the lattice of `gauge` in this engine, adding it if needed
-    int lattice_index(const hw_gauge *gauge, int *idx);
+    // index of the lattice entry of `gauge` for a fermion (EngFermion) in this engine,
+    // adding it if needed
+    int lattice_index(const hw_gauge *gauge, int *idx, int fermion = FERM_WILSON);
     // drop lattices with no used slot (compacts the tile list)
     int prune_lattices();
     int free_slots_on(int lat) const;
@@ -41,6 +43,7 @@ class Engine {
               int *slot, double diag = 1.0);
     double2 *own_b(int slot) { return bufs_[slot].b_own.as<double2>(); }
     double2 *own_x(int slot) { return bufs_[slot].x_own.as<double2>(); }
+    double2 *own_xfer(int slot) { return bufs_[slot].xfer.as<double2>(); }
     int ensure_own(int slot);
     // stream-ordered: run up to `iters` iterations of every running slot
     // (stops early when none runs)

@@ -139,6 +139,12 @@ struct hw_field {
     HalfBuf half[2];  // [0] EVEN, [1] ODD
 };
 
+// staggered colour-vector field (staggered.cu)
+struct hw_stag_field {
+    hw_lattice *lat = nullptr;
+    hw::DevBuf half[2];  // [0] EVEN, [1] ODD: 3 double2 planes each
+};
+
 namespace hw {
 int ensure_workspace(hw_lattice *lat);
 int ensure_reduction_capacity(hw_context *ctx, long nblocks);

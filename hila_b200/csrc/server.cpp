@@ -59,6 +59,7 @@ bool host_pinned(const void *p) {
 // cost more than the copy).
 class PinnedPool {
   public:
+    void set_keep_bytes(size_t b) { keep_bytes_ = b; }
     ~PinnedPool() {
         for (auto &e : free_) cudaFreeHost(e.second);
     }
@@ -81,7 +82,7 @@ class PinnedPool {
     void put(double *p, size_t n) {
         if (!p) return;
         std::lock_guard<std::mutex> lk(mu_);
-        if ((held_ + n) * sizeof(double) > kKeepBytes) {
+        if ((held_ + n) * sizeof(double) > keep_bytes_) {
             cudaFreeHost(p);
             return;
         }
@@ -90,7 +91,7 @@ class PinnedPool {
     }
 
   private:
-    static constexpr size_t kKeepBytes = size_t(4) << 30;  // idle buffers kept for reuse
+    size_t keep_bytes_ = size_t(16) << 30;  // idle buffers kept for reuse (hw_server_config.host_pool_bytes)
     std::mutex mu_;
     std::multimap<size_t, double *> free_;
     size_t held_ = 0;  // doubles in free_
@@ -115,9 +116,13 @@ struct Request {
     std::vector<const double *> src_direct;
     std::vector<double *> user_sol;
     std::vector<char> sol_direct;
-    // REQ_FIELDS: EVEN halves of the caller's device fields
+    // REQ_FIELDS: EVEN halves of the caller's device fields (Wilson or staggered)
     std::vector<double2 *> fb, fx;
+    int fermion = FERM_WILSON;
     uint64_t admit_chunk = 0, retire_chunk = 0;  // server chunks launched before admission / retirement
+    // entries of its lattice's staging ring holding sources copied to the device while
+    // the request waited for slots (host modes); empty: not staged
+    std::vector<int> stage;
     const double *source(int k) const {
         if (!src_direct.empty() && src_direct[k]) return src_direct[k];
         return pin[k] ? pin[k] : src[k].get();
@@ -200,10 +205,58 @@ struct hw_server {
     std::thread worker;
     std::string worker_error;
     uint64_t layout_launches = 0;  // AoS <-> SoA kernels of admit / retire
-    // Host <-> device copies and layout conversions of admitted / retired solves run on
-    // their own stream, ordered against the engine's stream by events, so they overlap
-    // the chunks of the other solves.
-    cudaStream_t copy_stream = nullptr;
+    // Host -> device copies and layout conversions of admitted solves run on in_stream,
+    // those of retired solves on out_stream, ordered against the engine's stream by
+    // events, so they overlap the chunks of the other solves and each other (the two
+    // copy directions use separate copy engines).  A retired solution is converted into
+    // its slot's staging buffer before it is copied out, so the slot can take a new
+    // source as soon as that conversion (conv_event) is done.
+    cudaStream_t in_stream = nullptr, out_stream = nullptr;
+    cudaEvent_t conv_event = nullptr;
+    bool conv_recorded = false;
+    // Sources of queued requests are copied to the device ahead of their admission, into
+    // a staging ring per gauge field (kEngMaxRhs source buffers, allocated the first time
+    // a request of that gauge field waits, kept until the server is destroyed), so the
+    // copies overlap the chunks of earlier requests.  An entry is free again as soon as
+    // the admission has enqueued its conversion: later copies into it follow on in_stream.
+    struct StageRing {
+        std::vector<std::unique_ptr<hw::DevBuf>> buf;
+        std::vector<int> free_list;
+    };
+    std::map<int, StageRing> rings;  // by gauge id
+    size_t ring_bytes = 0;           // device memory the rings hold (a ring is made only if it fits the budget)
+    void release_stage(hw::Request &q) {
+        if (q.stage.empty()) return;
+        StageRing &R = rings[q.gauge_id];
+        for (int e : q.stage) R.free_list.push_back(e);
+        q.stage.clear();
+    }
+    bool take_stage(hw::Request &q) {
+        auto it = rings.find(q.gauge_id);
+        if (it == rings.end()) {
+            const size_t bytes = q.n * sizeof(double), total = bytes * hw::kEngMaxRhs;
+            if (bytes_in_use + ring_bytes + total > cfg.hbm_budget_bytes) return false;
+            StageRing R;
+            for (int e = 0; e < hw::kEngMaxRhs; e++) {
+                R.buf.emplace_back(new hw::DevBuf());
+                if (R.buf[e]->alloc(bytes) != HW_OK) {
+                    hw::clear_error();
+                    return false;  // the DevBufs free what was allocated
+                }
+                R.free_list.push_back(hw::kEngMaxRhs - 1 - e);
+            }
+            ring_bytes += total;
+            it = rings.emplace(q.gauge_id, std::move(R)).first;
+        }
+        StageRing &R = it->second;
+        if ((int)R.free_list.size() < q.nrhs) return false;
+        for (int k = 0; k < q.nrhs; k++) {
+            q.stage.push_back(R.free_list.back());
+            R.free_list.pop_back();
+        }
+        return true;
+    }
+    const void *stage_ptr(const hw::Request &q, int k) { return rings[q.gauge_id].buf[q.stage[k]]->ptr; }
     std::vector<cudaEvent_t> free_events;
     struct Round {
         cudaEvent_t done;                                // solutions of `reqs` are on the host
@@ -238,6 +291,7 @@ int admit_waiting(hw_server *S) {
         std::shared_ptr<Request> q = *it;
         if (q->cancel) {
             it = S->queue.erase(it);
+            S->release_stage(*q);  // later copies into its entries follow its own on in_stream
             q->state = REQ_DONE;
             q->res.status = HW_ERR_CANCELLED;
             q->res.nrhs = q->nrhs;
@@ -247,7 +301,7 @@ int admit_waiting(hw_server *S) {
         }
         const GaugeEntry &G = S->gauges[q->gauge_id];
         int l;
-        int rc = E.lattice_index(G.gauge, &l);
+        int rc = E.lattice_index(G.gauge, &l, q->fermion);
         if (rc != HW_OK) return rc;
         if (std::find(blocked.begin(), blocked.end(), l) != blocked.end()) {
             ++it;
@@ -270,8 +324,10 @@ int admit_waiting(hw_server *S) {
             int slot;
             if (q->mode == REQ_FIELDS) {
                 // the engine reads b and accumulates x in the caller's fields (x: initial guess)
-                if ((rc = E.admit(l, q->kappa, q->fb[k], q->fx[k], q->tol, q->maxiters, S->cfg.delta,
-                                  ENG_MODE_SOLVE, &slot)) != HW_OK)
+                // staggered solves are FP64 throughout: a reliable update only confirms convergence
+                const double delta = q->fermion == FERM_STAGGERED ? 0.0 : S->cfg.delta;
+                if ((rc = E.admit(l, q->kappa, q->fb[k], q->fx[k], q->tol, q->maxiters, delta, ENG_MODE_SOLVE,
+                                  &slot)) != HW_OK)
                     return rc;
                 q->slots.push_back(slot);
                 continue;
@@ -283,13 +339,24 @@ int admit_waiting(hw_server *S) {
             // source: host (checkerboard AoS) -> the slot's x buffer as staging -> SoA b;
             // then x = 0, on the copy stream (the pageable source is staged by the
             // driver before the call returns, so it can be freed right after)
-            double *stage = reinterpret_cast<double *>(E.own_x(slot));
-            HW_CUDA(cudaMemcpyAsync(stage, q->source(k), q->n * sizeof(double), cudaMemcpyHostToDevice,
-                                    S->copy_stream));
-            launch_aos_to_soa((int)G.Vh, stage, HalfF64{E.own_b(slot), stride}, S->copy_stream);
+            if (S->conv_recorded) {  // the slot's x may still be read by a retire conversion
+                HW_CUDA(cudaStreamWaitEvent(S->in_stream, S->conv_event, 0));
+                S->conv_recorded = false;
+            }
+            const double *stage;
+            if (!q->stage.empty()) {  // copied ahead while the request waited
+                stage = static_cast<const double *>(S->stage_ptr(*q, k));
+            } else {
+                double *st = reinterpret_cast<double *>(E.own_x(slot));
+                HW_CUDA(cudaMemcpyAsync(st, q->source(k), q->n * sizeof(double), cudaMemcpyHostToDevice,
+                                        S->in_stream));
+                stage = st;
+            }
+            launch_aos_to_soa((int)G.Vh, stage, HalfF64{E.own_b(slot), stride}, S->in_stream);
             S->layout_launches++;
-            HW_CUDA(cudaMemsetAsync(E.own_x(slot), 0, (size_t)12 * stride * sizeof(double2), S->copy_stream));
+            HW_CUDA(cudaMemsetAsync(E.own_x(slot), 0, (size_t)12 * stride * sizeof(double2), S->in_stream));
         }
+        S->release_stage(*q);  // its conversions are enqueued: the entries can take new copies
         q->release_sources();
         q->state = REQ_RUNNING;
         S->running.push_back(q);
@@ -297,9 +364,18 @@ int admit_waiting(hw_server *S) {
     }
     if (admitted) {  // the next chunk starts after the new sources are in place
         cudaEvent_t e = S->event();
-        HW_CUDA(cudaEventRecord(e, S->copy_stream));
+        HW_CUDA(cudaEventRecord(e, S->in_stream));
         HW_CUDA(cudaStreamWaitEvent(S->ctx->stream, e, 0));
         S->free_events.push_back(e);
+    }
+    // copy the sources of the requests still queued (in arrival order) to the device now,
+    // behind the admissions above on the same stream, while the admitted solves run
+    for (const std::shared_ptr<Request> &q : S->queue) {
+        if (q->cancel || q->mode == REQ_FIELDS || !q->stage.empty()) continue;
+        if (!S->take_stage(*q)) continue;  // its ring is full: the next request may use another
+        for (int k = 0; k < q->nrhs; k++)
+            HW_CUDA(cudaMemcpyAsync(const_cast<void *>(S->stage_ptr(*q, k)), q->source(k), q->n * sizeof(double),
+                                    cudaMemcpyHostToDevice, S->in_stream));
     }
     return HW_OK;
 }
@@ -313,6 +389,12 @@ int retire_finished(hw_server *S) {
     Engine &E = *S->eng;
     hw_context *ctx = S->ctx;
     std::vector<std::shared_ptr<Request>> done;
+    struct Copy {
+        double *dst;
+        const double *src;
+        size_t bytes;
+    };
+    std::vector<Copy> copies;
     bool ordered = false;
     for (size_t n = 0; n < S->running.size();) {
         std::shared_ptr<Request> q = S->running[n];
@@ -333,7 +415,7 @@ int retire_finished(hw_server *S) {
             if (!ordered) {
                 cudaEvent_t e = S->event();
                 HW_CUDA(cudaEventRecord(e, ctx->stream));
-                HW_CUDA(cudaStreamWaitEvent(S->copy_stream, e, 0));
+                HW_CUDA(cudaStreamWaitEvent(S->out_stream, e, 0));
                 S->free_events.push_back(e);
                 ordered = true;
             }
@@ -365,11 +447,10 @@ int retire_finished(hw_server *S) {
                     dst = q->sol[k];
                 }
                 const int l = E.slot_lattice(slot);
-                double *stage = reinterpret_cast<double *>(E.own_b(slot));
-                launch_soa_to_aos((int)G.Vh, HalfF64{E.own_x(slot), E.lattice(l).stride}, stage, S->copy_stream);
+                double *stage = reinterpret_cast<double *>(E.own_xfer(slot));
+                launch_soa_to_aos((int)G.Vh, HalfF64{E.own_x(slot), E.lattice(l).stride}, stage, S->out_stream);
                 S->layout_launches++;
-                HW_CUDA(cudaMemcpyAsync(dst, stage, q->n * sizeof(double), cudaMemcpyDeviceToHost,
-                                        S->copy_stream));
+                copies.push_back({dst, stage, q->n * sizeof(double)});
             }
             S->stats.completed++;
             S->stats.solves_completed += q->nrhs;
@@ -384,10 +465,18 @@ int retire_finished(hw_server *S) {
         done.push_back(q);
         S->running.erase(S->running.begin() + n);
     }
+    if (!copies.empty()) {
+        // the slots' x buffers are free for new sources once these conversions are done;
+        // the copies to the host follow on the same stream
+        HW_CUDA(cudaEventRecord(S->conv_event, S->out_stream));
+        S->conv_recorded = true;
+        for (const Copy &c : copies)
+            HW_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, S->out_stream));
+    }
     if (!done.empty()) {
         hw_server::Round r;
         r.done = S->event();
-        HW_CUDA(cudaEventRecord(r.done, S->copy_stream));
+        HW_CUDA(cudaEventRecord(r.done, S->out_stream));
         r.reqs = std::move(done);
         S->retiring.push_back(std::move(r));
     }
@@ -441,6 +530,7 @@ void fail_all(hw_server *S, int rc) {
     }
     S->retiring.clear();
     for (auto &q : S->queue) {
+        S->release_stage(*q);
         q->res.status = rc;
         q->state = REQ_DONE;
     }
@@ -518,7 +608,10 @@ int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server 
     S->eng.reset(new Engine(ctx, cfg.precision == HW_PREC_F16 ? LOW_F16 : LOW_F32));
     int rc = S->eng->init();
     if (rc != HW_OK) return rc;
-    HW_CUDA(cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking));
+    HW_CUDA(cudaStreamCreateWithFlags(&S->in_stream, cudaStreamNonBlocking));
+    HW_CUDA(cudaStreamCreateWithFlags(&S->out_stream, cudaStreamNonBlocking));
+    HW_CUDA(cudaEventCreateWithFlags(&S->conv_event, cudaEventDisableTiming));
+    if (cfg.host_pool_bytes) S->pool.set_keep_bytes(cfg.host_pool_bytes);
     S->stats.bytes_budget = cfg.hbm_budget_bytes;
     hw_server *raw = S.get();
     S->worker = std::thread([raw] { server_loop(raw); });
@@ -536,13 +629,18 @@ int hw_server_destroy(hw_server *S) {
     if (S->worker.joinable()) S->worker.join();
     {
         std::lock_guard<std::recursive_mutex> glk(S->ctx->mu);
-        if (S->copy_stream) cudaStreamSynchronize(S->copy_stream);
+        cudaSetDevice(S->ctx->device);
+        for (cudaStream_t st : {S->in_stream, S->out_stream})
+            if (st) cudaStreamSynchronize(st);
+        S->rings.clear();  // the staging rings (streams synchronised above)
         S->eng.reset();
         for (auto &r : S->retiring) S->free_events.push_back(r.done);
         S->retiring.clear();
         for (cudaEvent_t e : S->free_events) cudaEventDestroy(e);
         S->free_events.clear();
-        if (S->copy_stream) cudaStreamDestroy(S->copy_stream);
+        for (cudaStream_t st : {S->in_stream, S->out_stream})
+            if (st) cudaStreamDestroy(st);
+        if (S->conv_event) cudaEventDestroy(S->conv_event);
     }
     delete S;
     return HW_OK;
@@ -649,19 +747,23 @@ int hw_server_submit(hw_server *S, int gauge_id, double kappa, int nrhs, const d
 
 int hw_server_submit_eo(hw_server *S, int gauge_id, double kappa, int nrhs, const double *const *sources,
                         double *const *solutions, double accuracy, int maxiters, uint64_t *request_id) {
-    HW_CHECK_ARG(S && sources && solutions && request_id, "null argument");
+    HW_CHECK_ARG(S && sources && request_id, "null argument");
     GaugeEntry G;
     int rc = submit_check(S, gauge_id, nrhs, accuracy, maxiters, &G);
     if (rc != HW_OK) return rc;
-    for (int k = 0; k < nrhs; k++) HW_CHECK_ARG(sources[k] && solutions[k], "source or solution %d is null", k);
+    for (int k = 0; k < nrhs; k++) HW_CHECK_ARG(sources[k], "source %d is null", k);
     std::shared_ptr<Request> q = new_request(S, G, gauge_id, kappa, nrhs, accuracy, maxiters, REQ_HOST_EO);
     q->src_direct.assign(nrhs, nullptr);
-    q->user_sol.assign(solutions, solutions + nrhs);
+    q->user_sol.assign(nrhs, nullptr);
+    if (solutions) q->user_sol.assign(solutions, solutions + nrhs);
     q->sol_direct.assign(nrhs, 0);
     for (int k = 0; k < nrhs; k++) {
-        q->sol_direct[k] = host_pinned(solutions[k]) ? 1 : 0;
+        q->sol_direct[k] = q->user_sol[k] && host_pinned(q->user_sol[k]) ? 1 : 0;
         if (host_pinned(sources[k])) {
             q->src_direct[k] = sources[k];  // read by DMA at admission
+            // the page-locked buffer that receives the solution is taken here, on the
+            // caller's thread, not by the server thread at retirement
+            if (!q->sol_direct[k]) q->pin[k] = S->pool.get(q->n);
             continue;
         }
         // pageable: one contiguous copy of the EVEN half into a page-locked buffer
@@ -693,6 +795,26 @@ int hw_server_submit_fields(hw_server *S, int gauge_id, double kappa, int nrhs, 
     return enqueue_request(S, G, q, request_id);
 }
 
+int hw_server_submit_staggered(hw_server *S, int gauge_id, double mass, int nrhs, const hw_stag_field *const *sources,
+                               hw_stag_field *const *solutions, double accuracy, int maxiters, uint64_t *request_id) {
+    HW_CHECK_ARG(S && sources && solutions && request_id, "null argument");
+    HW_CHECK_ARG(std::isfinite(mass) && mass != 0.0, "mass must be finite and nonzero");
+    GaugeEntry G;
+    int rc = submit_check(S, gauge_id, nrhs, accuracy, maxiters, &G);
+    if (rc != HW_OK) return rc;
+    std::shared_ptr<Request> q = new_request(S, G, gauge_id, mass, nrhs, accuracy, maxiters, REQ_FIELDS);
+    q->fermion = FERM_STAGGERED;
+    for (int k = 0; k < nrhs; k++) {
+        HW_CHECK_ARG(sources[k] && solutions[k], "source or solution field %d is null", k);
+        HW_CHECK_ARG(sources[k]->lat == G.gauge->lat && solutions[k]->lat == G.gauge->lat,
+                     "field %d belongs to another lattice than the gauge field", k);
+        HW_CHECK_ARG(sources[k] != solutions[k], "source and solution %d are the same field", k);
+        q->fb.push_back(const_cast<double2 *>(sources[k]->half[0].as<double2>()));
+        q->fx.push_back(solutions[k]->half[0].as<double2>());
+    }
+    return enqueue_request(S, G, q, request_id);
+}
+
 int hw_server_wait(hw_server *S, uint64_t request_id, double *const *solutions, double timeout_seconds,
                    hw_request_result *result) {
     HW_CHECK_ARG(S, "null argument");
@@ -712,9 +834,12 @@ int hw_server_wait(hw_server *S, uint64_t request_id, double *const *solutions, 
     const GaugeEntry G = S->gauges[q->gauge_id];
     lk.unlock();
     if (q->mode == REQ_HOST_EO && !q->sol.empty()) {
-        // solutions that could not be written by DMA (pageable arrays): the EVEN half
-        for (int k = 0; k < q->nrhs; k++)
-            if (!q->sol_direct[k] && q->sol[k]) std::memcpy(q->user_sol[k], q->sol[k], q->n * sizeof(double));
+        // solutions not written by DMA at retirement (pageable arrays, or arrays given only
+        // here): the EVEN half, in even-first order
+        for (int k = 0; k < q->nrhs; k++) {
+            double *dst = q->user_sol[k] ? q->user_sol[k] : (solutions ? solutions[k] : nullptr);
+            if (!q->sol_direct[k] && q->sol[k] && dst) std::memcpy(dst, q->sol[k], q->n * sizeof(double));
+        }
     } else if (q->mode == REQ_HOST_LEX && solutions && !q->sol.empty()) {
         for (int k = 0; k < q->nrhs; k++)
             if (solutions[k]) scatter_even(G, q->sol[k], solutions[k]);

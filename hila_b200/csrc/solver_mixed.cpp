@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "engine_host.h"
@@ -84,6 +85,65 @@ int mixed_solve(const hw_gauge *G, double kappa, const hw_field *src, hw_field *
     return status;
 }
 
+// Admit requests 0..n-1 in order as slots free up, run chunks of iterations for all
+// admitted slots, and collect each result as its slot finishes.  lattice_of(k, &l) finds
+// (or adds) request k's lattice entry, admit(k, l, &slot) starts it, finished(k) clears
+// what the solve leaves behind (enqueued before the slot is released).  Context lock held.
+int drive_batch(hw_context *ctx, Engine *E, int n, long max_chunks, hw_cg_result *results,
+                const std::function<int(int, int *)> &lattice_of, const std::function<int(int, int, int *)> &admit,
+                const std::function<cudaError_t(int)> &finished) {
+    std::vector<int> slot_of(n, -1), done(n, 0);
+    int next = 0, finished_n = 0, chunks = 0, rc;
+    // on an error, give back the slots still held by this batch
+    auto fail = [&](int code) {
+        for (int k = 0; k < next; k++)
+            if (!done[k] && slot_of[k] >= 0) E->release(slot_of[k]);
+        E->prune_lattices();
+        return code;
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    while (finished_n < n) {
+        // admit as many waiting requests as there are free slots (in order)
+        while (next < n) {
+            int l;
+            if ((rc = lattice_of(next, &l)) != HW_OK) return fail(rc);
+            if (E->free_slots_on(l) <= 0) break;
+            int slot;
+            if ((rc = admit(next, l, &slot)) != HW_OK) return fail(rc);
+            slot_of[next] = slot;
+            next++;
+        }
+        if ((rc = E->launch_chunk(16)) != HW_OK) return fail(rc);
+        chunks++;
+        if ((rc = E->read_states()) != HW_OK) return fail(rc);
+        const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        for (int k = 0; k < next; k++) {
+            if (done[k]) continue;
+            const EngState &s = E->state(slot_of[k]);
+            if (s.status == ENG_RUNNING) continue;
+            fill_result(s, now, chunks, &results[k]);
+            HW_CUDA(finished(k));
+            E->release(slot_of[k]);
+            done[k] = 1;
+            finished_n++;
+        }
+        E->prune_lattices();
+        if (chunks > max_chunks) {
+            set_error("batch solve did not finish within %ld chunks", max_chunks);
+            return fail(HW_ERR_TIMEOUT);
+        }
+        if (next == 0 && n > 0) {
+            set_error("batch solve could not admit any request");
+            return HW_ERR_INVALID;
+        }
+    }
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    int status = HW_OK;
+    for (int k = 0; k < n; k++)
+        if (results[k].status != HW_OK) status = results[k].status;
+    return status;
+}
+
 }  // namespace hw
 
 using namespace hw;
@@ -110,62 +170,48 @@ int hw_batch_solve(hw_context *ctx, int precision, double delta, const hw_solve_
     int rc;
     if ((rc = get_engine(ctx, precision == HW_PREC_F16 ? LOW_F16 : LOW_F32, &E)) != HW_OK) return rc;
     for (int k = 0; k < n; k++) tune_hop(reqs[k].gauge->lat, reqs[k].gauge);
-
-    std::vector<int> slot_of(n, -1), done(n, 0);
-    int next = 0, finished = 0, chunks = 0;
-    // on an error, give back the slots still held by this batch
-    auto fail = [&](int code) {
-        for (int k = 0; k < next; k++)
-            if (!done[k] && slot_of[k] >= 0) E->release(slot_of[k]);
-        E->prune_lattices();
-        return code;
-    };
     long max_chunks = 16;
     for (int k = 0; k < n; k++) max_chunks += reqs[k].maxiters / 16 + 2;
-    const auto t0 = std::chrono::steady_clock::now();
-    while (finished < n) {
-        // admit as many waiting requests as there are free slots (in order)
-        while (next < n) {
-            const hw_solve_request &q = reqs[next];
-            int l;
-            if ((rc = E->lattice_index(q.gauge, &l)) != HW_OK) return fail(rc);
-            if (E->free_slots_on(l) <= 0) break;
-            int slot;
-            if ((rc = E->admit(l, q.kappa, q.b->half[0].buf.as<double2>(), q.x->half[0].buf.as<double2>(),
-                               q.accuracy, q.maxiters, delta, ENG_MODE_SOLVE, &slot, 1.0 + q.hasenbusch_mh)) != HW_OK)
-                return fail(rc);
-            slot_of[next] = slot;
-            next++;
-        }
-        if ((rc = E->launch_chunk(16)) != HW_OK) return fail(rc);
-        chunks++;
-        if ((rc = E->read_states()) != HW_OK) return fail(rc);
-        const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        for (int k = 0; k < next; k++) {
-            if (done[k]) continue;
-            const EngState &s = E->state(slot_of[k]);
-            if (s.status == ENG_RUNNING) continue;
-            fill_result(s, now, chunks, &results[k]);
-            HW_CUDA(cudaMemsetAsync(reqs[k].x->half[1].buf.ptr, 0, reqs[k].x->half[1].buf.bytes, ctx->stream));
-            E->release(slot_of[k]);
-            done[k] = 1;
-            finished++;
-        }
-        E->prune_lattices();
-        if (chunks > max_chunks) {
-            set_error("batch solve did not finish within %ld chunks", max_chunks);
-            return fail(HW_ERR_TIMEOUT);
-        }
-        if (next == 0 && n > 0) {
-            set_error("batch solve could not admit any request");
-            return HW_ERR_INVALID;
-        }
+    return drive_batch(
+        ctx, E, n, max_chunks, results,
+        [&](int k, int *l) { return E->lattice_index(reqs[k].gauge, l); },
+        [&](int k, int l, int *slot) {
+            const hw_solve_request &q = reqs[k];
+            return E->admit(l, q.kappa, q.b->half[0].buf.as<double2>(), q.x->half[0].buf.as<double2>(), q.accuracy,
+                            q.maxiters, delta, ENG_MODE_SOLVE, slot, 1.0 + q.hasenbusch_mh);
+        },
+        [&](int k) { return cudaMemsetAsync(reqs[k].x->half[1].buf.ptr, 0, reqs[k].x->half[1].buf.bytes, ctx->stream); });
+}
+
+int hw_staggered_batch_solve(hw_context *ctx, const hw_stag_solve_request *reqs, int n, hw_cg_result *results) {
+    HW_CHECK_ARG(ctx && reqs && results && n >= 0, "null argument");
+    for (int k = 0; k < n; k++) {
+        const hw_stag_solve_request &q = reqs[k];
+        HW_CHECK_ARG(q.gauge && q.in && q.out, "request %d: null gauge or field", k);
+        HW_CHECK_ARG(q.gauge->lat->ctx == ctx, "request %d: gauge belongs to another context", k);
+        HW_CHECK_ARG(q.in->lat == q.gauge->lat && q.out->lat == q.gauge->lat, "request %d: lattice mismatch", k);
+        HW_CHECK_ARG(q.in != q.out, "request %d: in and out must differ", k);
+        HW_CHECK_ARG(q.accuracy > 0 && q.maxiters > 0, "request %d: bad accuracy or maxiters", k);
+        HW_CHECK_ARG(std::isfinite(q.mass) && q.mass != 0.0, "request %d: mass must be finite and nonzero", k);
     }
-    HW_CUDA(cudaStreamSynchronize(ctx->stream));
-    int status = HW_OK;
-    for (int k = 0; k < n; k++)
-        if (results[k].status != HW_OK) status = results[k].status;
-    return status;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    // staggered slots run their own FP64 phases in the engine that also serves FP16 Wilson solves
+    Engine *E;
+    int rc;
+    if ((rc = get_engine(ctx, LOW_F16, &E)) != HW_OK) return rc;
+    long max_chunks = 16;
+    for (int k = 0; k < n; k++) max_chunks += reqs[k].maxiters / 16 + 2;
+    return drive_batch(
+        ctx, E, n, max_chunks, results,
+        [&](int k, int *l) { return E->lattice_index(reqs[k].gauge, l, FERM_STAGGERED); },
+        [&](int k, int l, int *slot) {
+            const hw_stag_solve_request &q = reqs[k];
+            // FP64 throughout: a reliable update only confirms convergence (delta 0)
+            return E->admit(l, q.mass, q.in->half[0].as<double2>(), q.out->half[0].as<double2>(), q.accuracy,
+                            q.maxiters, 0.0, q.normal ? ENG_MODE_NORMAL : ENG_MODE_SOLVE, slot);
+        },
+        [&](int k) { return cudaMemsetAsync(reqs[k].out->half[1].ptr, 0, reqs[k].out->half[1].bytes, ctx->stream); });
 }
 
 int hw_engine_profile_enable(hw_context *ctx, int enable) {

@@ -16,12 +16,9 @@
 
 #include "hw_internal.h"
 #include "reduce.cuh"
+#include "staggered_math.cuh"
 #include "storage.cuh"
 
-struct hw_stag_field {
-    hw_lattice *lat = nullptr;
-    hw::DevBuf half[2];  // [0] EVEN, [1] ODD: 3 double2 planes each
-};
 
 namespace hw {
 namespace {
@@ -30,61 +27,8 @@ constexpr int kStagBlock = 128;
 constexpr int kStagVecBlock = 256;
 constexpr int kStagMaxBlocks = 1024;
 
-struct HalfStag {
-    double2 *p;
-    int stride;
-    __device__ __forceinline__ Cx<double> ld(int c, int i) const {
-        const double2 v = __ldg(p + (size_t)c * stride + i);
-        return {v.x, v.y};
-    }
-    __device__ __forceinline__ void st(int c, int i, Cx<double> v) const {
-        p[(size_t)c * stride + i] = make_double2(v.re, v.im);
-    }
-};
-
 HalfStag half_of(const hw_stag_field *f, int p) {
     return HalfStag{f->half[p].as<double2>(), f->lat->stride};
-}
-
-__device__ __forceinline__ double stag_eta(const int c[4], int d) {
-    int s = 0;
-    for (int k = 0; k < d; k++) s += c[k];
-    return (s & 1) ? 1.0 : -1.0;
-}
-
-// acc = sum_d eta_d(x) [U_d(x) v(x+d) - U_d(x-d)^dag v(x-d)] at checkerboard site i of parity par
-template <class Lk>
-__device__ __forceinline__ void stag_hop_site(const Geom &g, const Lk &U, int par, int i, const HalfStag &v,
-                                              Cx<double> acc[3]) {
-    const SiteNbrs n = site_neighbours(g, i, par);
-    int c[4];
-    site_coords(g, i, par, c);
-#pragma unroll
-    for (int a = 0; a < 3; a++) acc[a] = {0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        const double eta = stag_eta(c, d);
-        const double sf = (d == 3 && n.tfwd_wrap) ? -eta : eta;
-        const double sb = (d == 3 && n.tbwd_wrap) ? -eta : eta;
-        Su3<double> u;
-        U.load(par, d, i, u);
-        Cx<double> w[3];
-#pragma unroll
-        for (int b = 0; b < 3; b++) w[b] = v.ld(b, n.fwd[d]);
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            Cx<double> t = cmul(u.e[a][0], w[0]) + cmul(u.e[a][1], w[1]) + cmul(u.e[a][2], w[2]);
-            acc[a] = acc[a] + sf * t;
-        }
-        U.load(1 - par, d, n.bwd[d], u);
-#pragma unroll
-        for (int b = 0; b < 3; b++) w[b] = v.ld(b, n.bwd[d]);
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            Cx<double> t = cmul(conj(u.e[0][a]), w[0]) + cmul(conj(u.e[1][a]), w[1]) + cmul(conj(u.e[2][a]), w[2]);
-            acc[a] = acc[a] - sb * t;
-        }
-    }
 }
 
 // out = a * 0.5 SIGN acc  (x null)   or   out = m x + 0.5 SIGN acc

@@ -228,6 +228,13 @@ void hw_cg_params_default(hw_cg_params *params);
  * `out` holds the initial guess on entry. */
 int hw_cg_solve(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out,
                 const hw_cg_params *params, hw_cg_result *result);
+/* CG<Dirac_Wilson>::apply (conjugate_gradient.h:46-104 on the unpreconditioned operator,
+ * wilson.h:146-201, as test_CG.cpp:127-182 uses it): M^dag M out = in on ALL sites,
+ * out the initial guess, FP64 (params->precision must be HW_PREC_F64; NULL: defaults);
+ * stops when |r|^2 < accuracy^2 |in|^2 (with true_residual set, also on the recomputed
+ * |in - M^dag M out| / |in|, which result->true_residual reports). */
+int hw_wilson_cg_solve(const hw_gauge *gauge, double kappa, const hw_field *in, hw_field *out,
+                       const hw_cg_params *params, hw_cg_result *result);
 
 /* Solve M x = b on EVEN sites (M = Dirac_Wilson_evenodd) by CG on the normal
  * equations with source M^dagger b — the D (D^dag D)^{-1} D^dag pattern of
@@ -283,6 +290,7 @@ typedef struct hw_server_config {
     double delta;             /* reliable-update factor (<= 0: 0.005 for FP16, 1e-5 for FP32) */
     size_t hbm_budget_bytes;  /* device memory for solve slots (0: 80% of free memory at creation) */
     int chunk_iters;          /* CG iterations between admission points (<= 0: 8) */
+    size_t host_pool_bytes;   /* idle page-locked host buffers the server keeps for reuse (0: 16 GiB) */
 } hw_server_config;
 
 typedef struct hw_request_result {
@@ -324,7 +332,9 @@ int hw_server_submit(hw_server *server, int gauge_id, double kappa, int nrhs, co
  * of each solution written.  Page-locked arrays (cudaHostAlloc / cudaHostRegister)
  * are read and written by DMA directly: the caller keeps them valid and unread until
  * the request's wait returns.  Pageable sources are copied before the call returns;
- * pageable solutions are filled by hw_server_wait. */
+ * pageable solutions are filled by hw_server_wait.  `solutions` (or an entry) may be
+ * NULL: the solution is then copied by hw_server_wait into its `solutions` argument
+ * (EVEN half, even-first order) if one is given there. */
 int hw_server_submit_eo(hw_server *server, int gauge_id, double kappa, int nrhs, const double *const *sources,
                         double *const *solutions, double accuracy, int maxiters, uint64_t *request_id);
 /* queue M x = b for nrhs device fields of the gauge field's lattice (the form HILA's
@@ -334,11 +344,19 @@ int hw_server_submit_eo(hw_server *server, int gauge_id, double kappa, int nrhs,
  * caller leaves the fields alone until the request's wait returns. */
 int hw_server_submit_fields(hw_server *server, int gauge_id, double kappa, int nrhs, const hw_field *const *sources,
                             hw_field *const *solutions, double accuracy, int maxiters, uint64_t *request_id);
+/* queue the staggered solves M x = b (dirac_staggered_evenodd, staggered.h:193-279, at
+ * `mass`) for nrhs device colour-vector fields of the gauge field's lattice, in place as
+ * hw_server_submit_fields (solutions[k] holds the initial guess); FP64, batched with the
+ * server's other requests.  hw_stag_field: a staggered field (operator section below). */
+typedef struct hw_stag_field hw_stag_field;
+int hw_server_submit_staggered(hw_server *server, int gauge_id, double mass, int nrhs,
+                               const hw_stag_field *const *sources, hw_stag_field *const *solutions,
+                               double accuracy, int maxiters, uint64_t *request_id);
 /* wait up to timeout_seconds (< 0: forever) for a request; on completion copy
  * the solutions of an hw_server_submit request (canonical layout, ODD sites zero)
- * into solutions[0..nrhs-1] (solutions or an entry may be NULL; requests of the
- * other submit forms have their solutions in place and ignore it) and fill
- * *result.  HW_ERR_TIMEOUT if still running.  A finished request is forgotten
+ * into solutions[0..nrhs-1] (solutions or an entry may be NULL; field requests have
+ * their solutions in place, and hw_server_submit_eo requests use it only for the
+ * entries they were not given) and fill *result.  HW_ERR_TIMEOUT if still running.  A finished request is forgotten
  * after its wait. */
 int hw_server_wait(hw_server *server, uint64_t request_id, double *const *solutions, double timeout_seconds,
                    hw_request_result *result);
@@ -350,7 +368,7 @@ int hw_server_stats_get(hw_server *server, hw_server_stats *stats);
 
 /* Field<SU_vector<3,double>> for staggered fermions (libraries/dirac/staggered.h):
  * host layout double[V][3][2] (colour-vector complex, lexicographic). */
-typedef struct hw_stag_field hw_stag_field;
+/* hw_stag_field is declared with the serving entry points above */
 int hw_stag_field_create(hw_lattice *lat, hw_stag_field **field);  /* zero-filled */
 int hw_stag_field_destroy(hw_stag_field *field);
 int hw_stag_field_upload(hw_stag_field *field, const double *host, int parity);
@@ -367,6 +385,25 @@ int hw_staggered_evenodd_dagger(const hw_gauge *gauge, double mass, const hw_sta
  * :70-86, in the host link layout double[4][V][3][3][2].  Synchronises. */
 int hw_staggered_evenodd_force(const hw_gauge *gauge, double mass, const hw_stag_field *chi, const hw_stag_field *psi,
                                int sign, double *force);
+/* One staggered solve inside a batch (dirac_staggered_evenodd, staggered.h:193-279). */
+typedef struct hw_stag_solve_request {
+    const hw_gauge *gauge;     /* gauge field (selects the lattice) */
+    double mass;
+    const hw_stag_field *in;   /* right-hand side (EVEN) */
+    hw_stag_field *out;        /* solution (EVEN); holds the initial guess on entry */
+    double accuracy;           /* stop on the FP64-recomputed residual (below) <= accuracy */
+    int maxiters;
+    int normal;                /* 1: M^dag M out = in, CG<Op>::apply semantics (conjugate_gradient.h:46-104),
+                                  residual |in - M^dag M out| / |in|; 0: M out = in, residual
+                                  |in - M out| / |in| (CG on M^dag M with source M^dag in) */
+} hw_stag_solve_request;
+/* Many staggered solves on many lattices at once, on the same batched engine as the
+ * Wilson solves (no reference counterpart: HILA runs one CG<Op>::apply per source):
+ * FP64 CG in one kernel launch per phase for all admitted solves, up to 16 per lattice
+ * and 64 in total at a time; results[k] is request k's outcome (iterations,
+ * recomputed FP64 true residual); each solve gives bitwise the same result alone and
+ * in any batch, also beside Wilson solves of the same engine. */
+int hw_staggered_batch_solve(hw_context *ctx, const hw_stag_solve_request *requests, int n, hw_cg_result *results);
 /* CG<dirac_staggered_evenodd>::apply, conjugate_gradient.h:46-104: M^dag M out = in
  * on EVEN, out the initial guess; FP64 (params->precision must be HW_PREC_F64);
  * result reports the recomputed |in - M^dag M out| / |in|. */

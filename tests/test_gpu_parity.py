@@ -221,3 +221,21 @@ def test_golden_fixtures_gpu(hw, ctx, oracle):
     assert rel_site_err(fout.download(), g["apply"]) <= SITE_TOL
     D.dagger(fin, fout)
     assert rel_site_err(fout.download(), g["dagger"]) <= SITE_TOL
+
+
+@pytest.mark.parametrize("antiperiodic", [True, False])
+def test_unpreconditioned_cg(hw, ctx, oracle, antiperiodic):
+    """CG<Dirac_Wilson>::apply (hw_wilson_cg_solve): M^dag M x = b on ALL sites, judged by the
+    oracle's FP64 residual |b - M^dag M x| / |b| with M the unpreconditioned operator."""
+    dims = (4, 4, 4, 8)
+    U, lat, G = setup(hw, ctx, oracle, dims, seed=41, antiperiodic=antiperiodic)
+    b = oracle.gen_spinor(dims, 42, oracle.ALL)
+    D = hw.Dirac_Wilson(0.11, G)
+    fb, fx = hw.Field(lat, b), hw.Field(lat)
+    r = D.cg(fb, fx, accuracy=1e-11, true_residual=True)
+    assert r.converged, r
+    x = fx.download()
+    mx = oracle.wilson_apply(dims, U, 0.11, x, 1, antiperiodic)
+    mmx = oracle.wilson_apply(dims, U, 0.11, mx, -1, antiperiodic)
+    res = np.linalg.norm(mmx - b) / np.linalg.norm(b)
+    assert res <= 1e-10 and abs(res - r.true_residual) <= 1e-3 * res + 1e-15
