@@ -68,6 +68,8 @@ int Engine::init() {
     if ((rc = d_tickets_.alloc(sizeof(unsigned) * kEngMaxLat)) != HW_OK) return rc;
     if ((rc = d_ctl_.alloc(sizeof(int) * 8)) != HW_OK) return rc;
     if ((rc = d_work_.alloc(sizeof(unsigned long long) * kEngPhases * kEngWorkKinds)) != HW_OK) return rc;
+    if ((rc = d_sched_.alloc(sizeof(int) * kEngPhases)) != HW_OK) return rc;
+    HW_CUDA(cudaMemsetAsync(d_sched_.ptr, 0, d_sched_.bytes, ctx_->stream));
     HW_CUDA(cudaMemsetAsync(d_tickets_.ptr, 0, d_tickets_.bytes, ctx_->stream));
     HW_CUDA(cudaMemsetAsync(d_ctl_.ptr, 0, d_ctl_.bytes, ctx_->stream));
     HW_CUDA(cudaMemsetAsync(d_work_.ptr, 0, d_work_.bytes, ctx_->stream));
@@ -76,6 +78,9 @@ int Engine::init() {
     HW_CUDA(cudaMallocHost(&pinned_work_, d_work_.bytes));
     std::memset(pinned_work_, 0, d_work_.bytes);
     std::memset(&tables_, 0, sizeof(tables_));
+    // dynamic tile order of the inner phases (HW_ENGINE_SCHED=0: the static order)
+    tables_.dyn = 1;
+    if (const char *env = std::getenv("HW_ENGINE_SCHED")) tables_.dyn = std::atoi(env) != 0;
     for (int j = 0; j < kEngMaxProb; j++) {
         std::memset(&host_states_[j], 0, sizeof(EngState));
         host_states_[j].status = ENG_IDLE;
@@ -164,6 +169,7 @@ int Engine::prune_lattices() {
     if ((int)keep.size() == tables_.nlat) return HW_OK;
     EngTables nt;
     std::memset(&nt, 0, sizeof(nt));
+    nt.dyn = tables_.dyn;
     std::vector<const hw_gauge *> ng;
     std::vector<int> remap(tables_.nlat, -1);
     for (int l : keep) {
@@ -344,6 +350,7 @@ void Engine::set_ptrs() {
     ptrs_.tickets = d_tickets_.as<unsigned>();
     ptrs_.ctl = d_ctl_.as<int>();
     ptrs_.work = d_work_.as<unsigned long long>();
+    ptrs_.sched = d_sched_.as<int>();
 }
 
 int Engine::build_graph() {

@@ -391,10 +391,20 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
     __shared__ int s_na;
     __shared__ uint4 s_lx[STAGE ? 16 * kEngTile : 1];
     __shared__ unsigned s_lz[STAGE ? 8 * kEngTile : 1];
+    __shared__ int s_tile;
     const EngTables *T = P.T;
     const int ntiles = T->ntiles;
     const int max_tiles = T->max_tiles;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const bool dyn = T->dyn != 0;
+    // the next tile: block + k * grid, or the next value of the phase's counter; the
+    // partial sums are per (slot, tile), so the tile order does not change any result
+    auto next_tile = [&](int cur) {
+        if (!dyn) return cur + (int)gridDim.x;
+        if (threadIdx.x == 0) s_tile = atomicAdd(P.sched + PHASE, 1);
+        __syncthreads();
+        return s_tile;
+    };
+    for (int tile = dyn ? next_tile(0) : (int)blockIdx.x; tile < ntiles; tile = next_tile(tile)) {
         const int l = find_lattice(T, tile);
         const EngLattice &La = T->lat[l];
         const Geom g = La.g;
@@ -593,6 +603,8 @@ __global__ void __launch_bounds__(kEngTile) k_eng_vec(EngPtrs P) {
     if (PHASE == PH_R1 && *(volatile int *)(P.ctl + 2) == 0) return;
     const EngTables *T = P.T;
     const int ntiles = T->ntiles;
+    // static tile order: the vector phases are short and bound by DRAM, and the barriers of a
+    // dynamic order measured slower here (P5 0.176 -> 0.197 ms at 32^4, 12 sources)
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int l = find_lattice(T, tile);
         const EngLattice &La = T->lat[l];
@@ -662,6 +674,7 @@ __global__ void k_eng_control(EngPtrs P, int nprob, int chunk, cudaGraphConditio
         if (s.status == ENG_RUNNING) atomicAdd(&running, 1);
     }
     __syncthreads();
+    if (threadIdx.x < kEngPhases) P.sched[threadIdx.x] = 0;  // the next iteration's tile counters
     if (threadIdx.x == 0) {
         if (chunk <= 0) chunk = P.ctl[3];
         const int it = P.ctl[0] + 1;
@@ -673,7 +686,10 @@ __global__ void k_eng_control(EngPtrs P, int nprob, int chunk, cudaGraphConditio
     }
 }
 
-__global__ void k_eng_chunk_begin(EngPtrs P) { P.ctl[0] = 0; }
+__global__ void k_eng_chunk_begin(EngPtrs P) {
+    P.ctl[0] = 0;
+    for (int k = 0; k < kEngPhases; k++) P.sched[k] = 0;
+}
 
 // FP64 link planes (first six elements = rows 0 and 1) -> FP32 / FP16 12-real planes
 __global__ void k_eng_links(Geom g, const double2 *l64, int planes, int stride, float4 *l32, uint4 *l16a,

@@ -106,7 +106,8 @@ struct EngTables {
     int nlat;
     int ntiles;  // total tiles over all lattices
     int max_tiles;  // partial-sum stride: largest ntiles of any lattice
-    int pad;
+    int dyn;     // 1: the inner phases' blocks take tiles from a counter (balances lattices whose
+                 // tiles carry different numbers of active slots); 0: tile = block + k * grid
     EngLattice lat[kEngMaxLat];
     EngProblem prob[kEngMaxProb];
 };
@@ -121,6 +122,8 @@ struct EngPtrs {
                           // [2] reliable updates requested in this iteration,
                           // [3] iteration limit of a chunk (control kernel with chunk <= 0)
     unsigned long long *work;  // kEngPhases x kEngWorkKinds cumulative work units (below)
+    int *sched;           // kEngPhases tile counters of the inner phases' dynamic tile order
+                          // (zeroed at the start of a chunk and by every iteration's control kernel)
 };
 
 // Work units counted by every phase launch (cumulative, per phase), from which the

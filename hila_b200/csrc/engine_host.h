@@ -94,7 +94,7 @@ class Engine {
     long prof_n_[kEngPhases] = {};
     double prof_ms_[kEngPhases] = {};
     int launch_chunk_profiled(int iters);
-    DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_, d_work_;
+    DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_, d_work_, d_sched_;
     size_t partial_tiles_ = 0;
     EngGrid grid_{};
     EngPtrs ptrs_{};
