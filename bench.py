@@ -69,9 +69,9 @@ WORKLOADS = {
 ITERS_PER_SOLVE = {"cg": 59, "mrhs": 59, "cg8": None}
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k_eng_low<P4> launch per
-# output site, 12 FP16 sources with 18-real FP16 links: 999.2 MB over 165,888 sites in one ncu
+# output site, 12 FP16 sources with 18-real FP16 links: 1027.8 MB over 165,888 sites in one ncu
 # capture at 24^4; every array is read once, so it scales with the sites.
-P4_TRAFFIC_PER_SITE_12 = 999.2e6 / 165888
+P4_TRAFFIC_PER_SITE_12 = 1027.8e6 / 165888
 
 # DRAM traffic of the two k_hop launches of one even-odd apply (12-real FP64 links), per
 # output site: 633.6 MB + 865.3 MB over 524,288 sites in one ncu capture at 32^4; every
