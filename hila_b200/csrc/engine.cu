@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
     __shared__ uint4 s_lx[STAGE ? 16 * kEngTile : 1];
     __shared__ unsigned s_lz[STAGE ? 8 * kEngTile : 1];
     __shared__ int s_tile;
+    __shared__ double s_red[NRED > 0 ? kEngMaxRhs : 1][kEngTile / 32];
     const EngTables *T = P.T;
     const int ntiles = T->ntiles;
     const int max_tiles = T->max_tiles;
@@ -498,14 +499,24 @@ __global__ void __launch_bounds__(kEngTile, MINB) k_eng_low(EngPtrs P) {
                     const int j = s_act[g0 + r];
                     double red[2] = {0.0, 0.0};
                     if (valid) epi_low<PHASE, LOW>(T->prob[j], P.S[j], stride, i, acc[r], red);
-                    // the block-wide sum per slot also keeps the warps of a block on the
-                    // same slot (neighbour reads shared in L1; measured faster than one
-                    // barrier per tile)
+                    // each warp keeps its sum in shared memory; the slots' sums are formed
+                    // once per tile below, in block_sum's order (one barrier per tile
+                    // instead of two per slot)
                     if constexpr (NRED > 0) {
-                        double sum = block_sum<kEngTile>(red[0], smem);
-                        if (threadIdx.x == 0) P.partials[((size_t)j * 2) * max_tiles + lt] = sum;
+                        const double v = warp_sum(red[0]);
+                        if ((threadIdx.x & 31) == 0) s_red[g0 + r][threadIdx.x >> 5] = v;
                     }
                 }
+            }
+        }
+        if constexpr (NRED > 0) {
+            __syncthreads();
+            if (threadIdx.x < na) {
+                double sum = 0;
+#pragma unroll
+                for (int w = 0; w < kEngTile / 32; w++) sum += s_red[threadIdx.x][w];
+                P.partials[((size_t)s_act[threadIdx.x] * 2) * max_tiles + lt] = sum;
+                __threadfence();  // visible before the lattice's ticket is taken
             }
         }
         __syncthreads();  // s_act is rewritten by the next tile
