@@ -462,6 +462,16 @@ def run_ours(args, dist: Dist):
         ctx.engine_profile(False)
         result["phases"] = phase_table(prof, prec, args.link_format, peak)
         engine_roof = result["phases"]["P4"]
+        # the launch-shape tuner's entry for this batch (its work class: bit length of the
+        # solves x 128-site tiles of the lattice), timed during the warm-up steps
+        cls = (nrhs * -(-(V // 2) // 128)).bit_length()
+        ent = next((t for t in ctx.engine_tuning(prec) if t["work_class"] == cls), None)
+        if ent is not None:
+            result["tuner"] = {
+                "work_class": cls,
+                "shapes": [{"variant": v, "dynamic_order": d, "ms_per_iteration": round(ms, 4), "samples": n}
+                           for v, d, ms, n in ent["shapes"]],
+                "chosen": ent["chosen"]}
         if not args.no_served and dist.world == 1:
             # the same 32^4 workload through the continuous-batching server (serve32: 32 requests of
             # 12 sources arriving faster than they are served), against the plain FP64 CG serving

@@ -90,6 +90,12 @@ class _EngineProfile(ctypes.Structure):
                 ("work", (ctypes.c_uint64 * 4) * 12)]
 
 
+class _EngineTuning(ctypes.Structure):
+    _fields_ = [("work_class", ctypes.c_int), ("nshapes", ctypes.c_int), ("variant", ctypes.c_int * 4),
+                ("dynamic_order", ctypes.c_int * 4), ("ms_per_iteration", ctypes.c_double * 4),
+                ("samples", ctypes.c_int * 4), ("chosen", ctypes.c_int)]
+
+
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("cancelled", ctypes.c_uint64), ("running", ctypes.c_uint64), ("queued", ctypes.c_uint64),
@@ -125,6 +131,7 @@ _SIGNATURES = {
     "hw_context_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "hw_engine_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
     "hw_engine_profile_get": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "hw_engine_tuning_get": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "hw_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "hw_host_free": (ctypes.c_int, [_vp]),
     "hw_lattice_create": (ctypes.c_int, [_vp, _ip, ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -339,6 +346,21 @@ class Context:
         _check(lib().hw_engine_profile_get(self.handle, PRECISIONS[precision], ctypes.byref(out)))
         return {name: (out.launches[k], out.ms[k], tuple(int(v) for v in out.work[k]))
                 for k, name in enumerate(self.ENGINE_PHASES)}
+
+    def engine_tuning(self, precision: str = "f16") -> list:
+        """The launch-shape tuner's entries of one engine (hw_engine_tuning_get), by work class:
+        [{"work_class", "shapes": [(variant, dynamic_order, ms_per_iteration, samples)],
+        "chosen": index or None}]."""
+        out = (_EngineTuning * 64)()
+        n = ctypes.c_int(0)
+        _check(lib().hw_engine_tuning_get(self.handle, PRECISIONS[precision], out, 64, ctypes.byref(n)))
+        res = []
+        for t in out[:n.value]:
+            shapes = [(t.variant[c], t.dynamic_order[c], t.ms_per_iteration[c], t.samples[c])
+                      for c in range(t.nshapes)]
+            res.append({"work_class": t.work_class, "shapes": shapes,
+                        "chosen": t.chosen if t.chosen >= 0 else None})
+        return res
 
     def stream(self) -> int:
         """The library's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

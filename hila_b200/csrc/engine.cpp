@@ -58,6 +58,8 @@ Engine::~Engine() {
     if (pinned_work_) cudaFreeHost(pinned_work_);
     for (cudaEvent_t e : prof_ev_)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : tune_ev_)
+        if (e) cudaEventDestroy(e);
 }
 
 int Engine::init() {
@@ -78,9 +80,8 @@ int Engine::init() {
     HW_CUDA(cudaMallocHost(&pinned_work_, d_work_.bytes));
     std::memset(pinned_work_, 0, d_work_.bytes);
     std::memset(&tables_, 0, sizeof(tables_));
-    // dynamic tile order of the inner phases (HW_ENGINE_SCHED=0: the static order)
+    // dynamic tile order of the inner phases until launch_chunk picks the chunk's shape
     tables_.dyn = 1;
-    if (const char *env = std::getenv("HW_ENGINE_SCHED")) tables_.dyn = std::atoi(env) != 0;
     for (int j = 0; j < kEngMaxProb; j++) {
         std::memset(&host_states_[j], 0, sizeof(EngState));
         host_states_[j].status = ENG_IDLE;
@@ -394,7 +395,7 @@ int Engine::configure() {
     }
     if (mask == 0) mask = 1;
     if (fermions == 0) fermions = 1;
-    int variant = default_variant();
+    int variant = want_variant_ ? want_variant_ : default_variant();
     if (const char *env = std::getenv("HW_ENGINE_VARIANT")) variant = std::atoi(env);
     // launch shapes (engine.cu): 2 for both precisions, 4 and 7 for FP16 only; the
     // tensor-core variant 4 reads the 18-real FP16 links, which exist only with full18_
@@ -413,10 +414,61 @@ int Engine::configure() {
     return HW_OK;
 }
 
+// HW_ENGINE_TUNE=0 turns the tuner off; a shape or tile order forced by HW_ENGINE_VARIANT
+// or HW_ENGINE_SCHED is not tuned (read at every chunk)
+int Engine::tune_shapes(const TuneShape **shapes) const {
+    static const TuneShape f16[] = {{7, 1}, {2, 1}, {7, 0}, {2, 0}};
+    static const TuneShape f32[] = {{2, 1}, {2, 0}};
+    if (const char *env = std::getenv("HW_ENGINE_TUNE"))
+        if (std::atoi(env) == 0) return 0;
+    if (std::getenv("HW_ENGINE_VARIANT") || std::getenv("HW_ENGINE_SCHED")) return 0;
+    *shapes = low_ == LOW_F16 ? f16 : f32;
+    return low_ == LOW_F16 ? 4 : 2;
+}
+
+int Engine::work_class() const {
+    unsigned long long units = 0;
+    for (int j = 0; j < kEngMaxProb; j++) {
+        if (!slots_[j].used || host_states_[j].status != ENG_RUNNING) continue;
+        const EngLattice &L = tables_.lat[slots_[j].lat];
+        if (L.fermion == FERM_WILSON) units += (unsigned long long)L.ntiles;
+    }
+    int bits = 0;
+    while (units) {
+        bits++;
+        units >>= 1;
+    }
+    return bits;
+}
+
 int Engine::launch_chunk(int iters) {
     int rc;
+    // the chunk's shape: forced by the environment, the tuner's for this work class (a
+    // candidate still being timed, or the fastest), or the default
+    const TuneShape *shapes = nullptr;
+    const int nshapes = tune_shapes(&shapes);
+    int cls = 0, shape = -1, dyn = 1;
+    want_variant_ = 0;
+    if (const char *env = std::getenv("HW_ENGINE_SCHED")) dyn = std::atoi(env) != 0;
+    if (nshapes > 1 && (cls = work_class()) > 0) {
+        TuneEntry &e = tune_[cls];
+        shape = e.chosen >= 0 ? e.chosen : e.next;
+        want_variant_ = shapes[shape].variant;
+        dyn = shapes[shape].dyn;
+        if (e.chosen >= 0 || ctx_->engine_profile) cls = 0;  // decided, or profiling: no timing
+    }
+    if (tables_.dyn != dyn) {
+        tables_.dyn = dyn;
+        tables_dirty_ = true;
+    }
     if ((rc = configure()) != HW_OK) return rc;
     if ((rc = ensure_partials()) != HW_OK) return rc;
+    if (cls > 0) {
+        if ((rc = upload_tables()) != HW_OK) return rc;
+        tune_pending_.cls = cls;
+        tune_pending_.shape = shape;
+        return launch_chunk_timed(iters);
+    }
     if (use_graph_ && !chunk_exec_ && (rc = build_graph()) != HW_OK) return rc;
     if ((rc = upload_tables()) != HW_OK) return rc;
     if (ctx_->engine_profile) return launch_chunk_profiled(iters);
@@ -434,6 +486,65 @@ int Engine::launch_chunk(int iters) {
     HW_CUDA(cudaMemcpyAsync(d_ctl_.as<int>() + 3, &iters, sizeof(int), cudaMemcpyHostToDevice, ctx_->stream));
     HW_CUDA(cudaGraphLaunch(chunk_exec_, ctx_->stream));
     return HW_OK;
+}
+
+// A chunk of the tuner: the iterations from the host (no graph) with events around the
+// phases of the first kTuneMaxIters; read_states turns them into a sample.
+int Engine::launch_chunk_timed(int iters) {
+    if (tune_ev_.empty()) {
+        tune_ev_.assign((size_t)kTuneMaxIters * (kEngPhases + 1), nullptr);
+        for (cudaEvent_t &e : tune_ev_) HW_CUDA(cudaEventCreate(&e));
+    }
+    int running = 0;
+    for (int j = 0; j < kEngMaxProb; j++) running += slots_[j].used && host_states_[j].status == ENG_RUNNING;
+    tune_pending_.running = running;
+    tune_pending_.iters = iters < kTuneMaxIters ? iters : kTuneMaxIters;
+    set_ptrs();
+    eng_enqueue_chunk_begin(ptrs_, ctx_->stream);
+    for (int k = 0; k < iters; k++) {
+        const cudaEvent_t *ev = k < tune_pending_.iters ? &tune_ev_[(size_t)k * (kEngPhases + 1)] : nullptr;
+        eng_enqueue_iteration(low_, ptrs_, grid_, ctx_->stream, ev);
+        eng_enqueue_control(ptrs_, kEngMaxProb, iters, 0, 0, ctx_->stream);
+    }
+    HW_CUDA(cudaGetLastError());
+    return HW_OK;
+}
+
+// After the synchronisation of read_states: a timed chunk in which every solve ran all
+// its iterations (none finished, so no iteration was partly idle) gives a sample.
+void Engine::tune_collect() {
+    const int cls = tune_pending_.cls, shape = tune_pending_.shape, n = tune_pending_.iters;
+    tune_pending_.cls = -1;
+    if (cls <= 0 || n <= 0) return;
+    int running = 0;
+    for (int j = 0; j < kEngMaxProb; j++) running += slots_[j].used && host_states_[j].status == ENG_RUNNING;
+    TuneEntry &e = tune_[cls];
+    if (running != tune_pending_.running) return;  // the next chunk times the same candidate
+    std::vector<double> it(n);
+    for (int k = 0; k < n; k++) {
+        const cudaEvent_t *ev = &tune_ev_[(size_t)k * (kEngPhases + 1)];
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, ev[0], ev[PH_R1]) != cudaSuccess ||
+            cudaEventElapsedTime(&b, ev[PH_P5], ev[kEngPhases]) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        it[k] = (double)a + (double)b;
+    }
+    std::sort(it.begin(), it.end());
+    const double med = it[n / 2];
+    if (e.samples[shape] == 0 || med < e.ms[shape]) e.ms[shape] = med;
+    e.samples[shape]++;
+    const TuneShape *shapes = nullptr;
+    const int ns = tune_shapes(&shapes);
+    if (ns <= 0) return;
+    e.next = (shape + 1) % ns;
+    int best = 0;
+    for (int c = 0; c < ns; c++) {
+        if (e.samples[c] < kTuneSamples) return;
+        if (e.ms[c] < e.ms[best]) best = c;
+    }
+    e.chosen = best;
 }
 
 // Host-loop chunk with events around every phase; synchronises after each
@@ -504,6 +615,7 @@ int Engine::read_states() {
     bodies_total_ = reinterpret_cast<const unsigned long long *>(pinned_ctl_ + 6)[0];
     for (int j = 0; j < kEngMaxProb; j++)
         if (slots_[j].used) host_states_[j] = pinned_states_[j];
+    tune_collect();
     return HW_OK;
 }
 

@@ -1,6 +1,7 @@
 // Host side of the batched mixed-precision CG engine (kernels in engine.cu).
 #pragma once
 
+#include <map>
 #include <vector>
 
 #include "engine.h"
@@ -19,6 +20,26 @@ struct SlotBuffers {
 struct SlotInfo {
     bool used = false;
     int lat = -1;
+};
+
+// Online choice of the inner phases' launch shape.  The candidates round every product
+// and sum alike (the packed two-solve hop and the one-solve-per-thread hop, each with
+// the dynamic or the static tile order), so a solve's bits do not depend on the choice.
+// Each is timed on real iterations of the running batch (median over a chunk of the
+// device time of P1..P4 and P5, which the shape changes; the reliable-update phases do
+// not depend on it) and the fastest is kept per work class.
+struct TuneShape {
+    int variant;  // EngGrid::variant
+    int dyn;      // EngTables::dyn
+};
+constexpr int kTuneMaxShapes = 4;
+constexpr int kTuneSamples = 2;   // timed chunks per candidate
+constexpr int kTuneMaxIters = 16;  // iterations of a chunk with events
+struct TuneEntry {
+    double ms[kTuneMaxShapes] = {};  // lowest median per-iteration time seen
+    int samples[kTuneMaxShapes] = {};
+    int next = 0;     // candidate of the next timed chunk
+    int chosen = -1;  // index of the fastest, once every candidate has its samples
 };
 
 class Engine {
@@ -68,6 +89,13 @@ class Engine {
     int nlat() const { return tables_.nlat; }
     const hw_gauge *gauge(int l) const { return gauges_[l]; }
     int upload_tables();
+    // launch-shape candidates of this engine (empty when a shape is forced by the
+    // environment or tuning is off) and the tuner's entries by work class
+    int tune_shapes(const TuneShape **shapes) const;
+    const std::map<int, TuneEntry> &tuning() const { return tune_; }
+    // work class of the running Wilson solves: bit length of the sum over them of
+    // their lattice's tiles (0: none)
+    int work_class() const;
 
   private:
     int ensure_slot_buffers(int slot, int stride);
@@ -94,6 +122,14 @@ class Engine {
     long prof_n_[kEngPhases] = {};
     double prof_ms_[kEngPhases] = {};
     int launch_chunk_profiled(int iters);
+    int launch_chunk_timed(int iters);
+    void tune_collect();
+    int want_variant_ = 0;  // the tuner's shape for the next chunks (0: the default)
+    std::map<int, TuneEntry> tune_;
+    std::vector<cudaEvent_t> tune_ev_;  // kTuneMaxIters x (kEngPhases + 1)
+    struct {
+        int cls = -1, shape = -1, iters = 0, running = 0;
+    } tune_pending_;
     DevBuf d_tables_, d_states_, d_partials_, d_tickets_, d_ctl_, d_work_, d_sched_;
     size_t partial_tiles_ = 0;
     EngGrid grid_{};

@@ -235,4 +235,32 @@ int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out
     return HW_OK;
 }
 
+int hw_engine_tuning_get(hw_context *ctx, int precision, hw_engine_tuning *out, int max, int *n) {
+    HW_CHECK_ARG(ctx && n && (out || max <= 0), "null argument");
+    HW_CHECK_ARG(precision == HW_PREC_F32 || precision == HW_PREC_F16, "precision must be HW_PREC_F32 or HW_PREC_F16");
+    static_assert(HW_TUNE_MAX_SHAPES == kTuneMaxShapes, "tuner shapes");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    *n = 0;
+    Engine *e = ctx->engines[low_of(precision)];
+    if (!e) return HW_OK;
+    const TuneShape *shapes = nullptr;
+    const int ns = e->tune_shapes(&shapes);
+    if (ns <= 0) return HW_OK;
+    for (const auto &kv : e->tuning()) {
+        if (*n >= max) break;
+        hw_engine_tuning &t = out[(*n)++];
+        std::memset(&t, 0, sizeof(t));
+        t.work_class = kv.first;
+        t.nshapes = ns;
+        for (int c = 0; c < ns; c++) {
+            t.variant[c] = shapes[c].variant;
+            t.dynamic_order[c] = shapes[c].dyn;
+            t.ms_per_iteration[c] = kv.second.samples[c] ? kv.second.ms[c] : 0.0;
+            t.samples[c] = kv.second.samples[c];
+        }
+        t.chosen = kv.second.chosen;
+    }
+    return HW_OK;
+}
+
 }  // extern "C"

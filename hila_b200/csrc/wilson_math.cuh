@@ -44,10 +44,14 @@ template <typename R>
 __device__ __forceinline__ Cx<R> mul_i(Cx<R> a) {
     return {-a.im, a.re};
 }
-// a * b
+// a product rounded on its own (never contracted into a following add)
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+// a * b: the products by a.re rounded, then the a.im terms fused.  The order is fixed
+// (and is the one of the packed two-solve hop), so every launch shape rounds alike.
 template <typename R>
 __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
-    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    return {fma(-a.im, b.im, mul_rn(a.re, b.re)), fma(a.im, b.re, mul_rn(a.re, b.im))};
 }
 // acc + a * b
 template <typename R>
@@ -112,8 +116,8 @@ template <typename R>
 __device__ __forceinline__ void su3_adj_mul(const Su3<R> &u, const Cx<R> h[3], Cx<R> v[3]) {
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        Cx<R> a = {u.e[0][i].re * h[0].re + u.e[0][i].im * h[0].im,
-                   u.e[0][i].re * h[0].im - u.e[0][i].im * h[0].re};
+        Cx<R> a = {fma(u.e[0][i].im, h[0].im, mul_rn(u.e[0][i].re, h[0].re)),
+                   fma(-u.e[0][i].im, h[0].re, mul_rn(u.e[0][i].re, h[0].im))};
         a = cjmadd(a, u.e[1][i], h[1]);
         a = cjmadd(a, u.e[2][i], h[2]);
         v[i] = a;

@@ -442,6 +442,28 @@ int hw_engine_profile_enable(hw_context *ctx, int enable);
 /* counters of the engine of one precision (HW_PREC_F32 / HW_PREC_F16); zeros if it has not run */
 int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out);
 
+/* The launch-shape tuner of the batched engines (no reference counterpart).  The inner
+ * phases have launch shapes that round every product and sum alike: two solves per
+ * thread in packed FP32 or one, each with tiles taken from a counter or in a fixed
+ * order.  An engine times them on chunks of real iterations of the running solves
+ * (median device time per iteration of P1..P4 and P5) and keeps the fastest per work
+ * class, the bit length of the sum over the running Wilson solves of their lattice's
+ * 128-site tiles.  A solve's result does not depend on the shape.  HW_ENGINE_TUNE=0
+ * turns the tuner off; HW_ENGINE_VARIANT or HW_ENGINE_SCHED force a shape instead. */
+#define HW_TUNE_MAX_SHAPES 4
+typedef struct hw_engine_tuning {
+    int work_class;
+    int nshapes;                                  /* candidates of this engine */
+    int variant[HW_TUNE_MAX_SHAPES];              /* launch shape (HW_ENGINE_VARIANT values) */
+    int dynamic_order[HW_TUNE_MAX_SHAPES];        /* 1: tiles from a counter; 0: fixed order */
+    double ms_per_iteration[HW_TUNE_MAX_SHAPES];  /* lowest median seen; 0: not timed yet */
+    int samples[HW_TUNE_MAX_SHAPES];              /* timed chunks */
+    int chosen;                                   /* index of the kept shape; -1 while timing */
+} hw_engine_tuning;
+/* Up to max entries, by increasing work class, of the engine of one precision; *n is the
+ * number written (0 if the engine has not run or the tuner is off). */
+int hw_engine_tuning_get(hw_context *ctx, int precision, hw_engine_tuning *out, int max, int *n);
+
 /* ------------------------------------------------------------------ inputs */
 
 /* Seeded synthetic inputs (no reference counterpart beyond hila::seed_random

@@ -163,8 +163,8 @@ def test_engine_launch_shapes(hw, ctx, oracle, variant, monkeypatch):
     """Every launch shape the FP16 engine keeps (HW_ENGINE_VARIANT: 2 one source per thread,
     4 the tensor-core hop, 7 the packed default): a batch of three sources on two lattices
     converges to true residual 1e-10 by the oracle, and each solve is bitwise the same alone
-    as in the batch.  The shapes differ in how products are rounded, so solutions of
-    different shapes are compared only through the true residual."""
+    as in the batch.  The tensor-core shape sums its products in another order, so its
+    solutions are compared with the others only through the true residual."""
     monkeypatch.setenv("HW_ENGINE_VARIANT", str(variant))
     specs = [((8, 8, 8, 8), 81, 0.124), ((4, 4, 4, 8), 82, 0.12)]
     built = []
@@ -185,3 +185,64 @@ def test_engine_launch_shapes(hw, ctx, oracle, variant, monkeypatch):
         [ra] = hw.batch_solve(ctx, [(D, fb, alone, TOL)], precision="f16")
         assert ra.iterations == r.iterations
         assert np.array_equal(alone.download(), x), variant
+
+
+def test_engine_shapes_round_alike(hw, ctx, oracle, monkeypatch):
+    """The one-source-per-thread shape (2) and the packed two-source default (7) round every
+    product and sum in the same order: a batch gives bitwise the same solutions and
+    iteration counts in both, so the shape can be chosen by speed alone."""
+    specs = [((8, 8, 8, 8), 83, 0.124), ((4, 4, 4, 8), 84, 0.12)]
+    work = []
+    for n, (dims, seed, kappa) in enumerate(specs):
+        U, lat, G = make(hw, ctx, oracle, dims, seed)
+        D = hw.Dirac_Wilson_evenodd(kappa, G)
+        for k in range(3 if n == 0 else 2):
+            b = oracle.gen_spinor(dims, 300 + 10 * n + k, oracle.EVEN)
+            work.append((lat, D, hw.Field(lat, b)))
+    out = {}
+    for variant in (7, 2):
+        monkeypatch.setenv("HW_ENGINE_VARIANT", str(variant))
+        xs = [hw.Field(lat) for (lat, _, _) in work]
+        res = hw.batch_solve(ctx, [(D, fb, x, TOL) for (_, D, fb), x in zip(work, xs)], precision="f16")
+        assert all(r.converged for r in res)
+        out[variant] = ([r.iterations for r in res], [x.download() for x in xs])
+    assert out[7][0] == out[2][0]
+    for a, b in zip(out[7][1], out[2][1]):
+        assert np.array_equal(a, b)
+
+
+def test_engine_tuner(hw, ctx, oracle, monkeypatch):
+    """The launch-shape tuner times its candidate shapes on the running solves, keeps the
+    fastest for the work class, and the solves it switches shapes under give bitwise the
+    same results as with one shape forced."""
+    for k in ("HW_ENGINE_VARIANT", "HW_ENGINE_SCHED", "HW_ENGINE_TUNE"):
+        monkeypatch.delenv(k, raising=False)
+    dims, kappa = (12, 12, 12, 12), 0.122
+    U, lat, G = make(hw, ctx, oracle, dims, 85)
+    D = hw.Dirac_Wilson_evenodd(kappa, G)
+    bs = [hw.Field(lat, oracle.gen_spinor(dims, 400 + k, oracle.EVEN)) for k in range(5)]
+
+    def solve():
+        xs = [hw.Field(lat) for _ in bs]
+        res = hw.batch_solve(ctx, [(D, fb, x, TOL) for fb, x in zip(bs, xs)], precision="f16")
+        assert all(r.converged for r in res)
+        return [r.iterations for r in res], [x.download() for x in xs]
+
+    # 5 solves x 81 tiles of 12^4: work class 9
+    first = solve()
+    entry = None
+    for _ in range(12):
+        entry = next((t for t in ctx.engine_tuning("f16") if t["work_class"] == 9), None)
+        if entry is not None and entry["chosen"] is not None:
+            break
+        again = solve()
+        assert again[0] == first[0]
+        assert all(np.array_equal(a, b) for a, b in zip(again[1], first[1]))
+    assert entry is not None and entry["chosen"] is not None, entry
+    assert {(v, d) for v, d, _, _ in entry["shapes"]} == {(7, 1), (2, 1), (7, 0), (2, 0)}
+    assert all(ms > 0 and n >= 2 for _, _, ms, n in entry["shapes"])
+    monkeypatch.setenv("HW_ENGINE_VARIANT", "2")
+    monkeypatch.setenv("HW_ENGINE_SCHED", "0")
+    forced = solve()
+    assert forced[0] == first[0]
+    assert all(np.array_equal(a, b) for a, b in zip(forced[1], first[1]))
