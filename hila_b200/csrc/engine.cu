@@ -862,6 +862,8 @@ void enqueue_iteration_mma(const EngPtrs &P, const EngGrid &G, cudaStream_t s, c
 //   7: FP16 only, the default: P1, P3 with two right-hand sides per thread in the lanes of
 //      packed FP32 instructions (pair.cuh), <= 168 registers (3 blocks); P2, P4 and the
 //      reliable update as variant 2
+// 2 and 7 round every operation alike (same bits); the engine's tuner picks between them
+// by timing (engine.cpp).  4 sums its products in another order.
 // (one right-hand side per thread at 4 or 5 blocks per SM, two per thread sharing the links
 // without packing, packed P1..P4, packed P1..P3, and P1/P3 streaming their neighbour data
 // through a cp.async ring in shared memory were measured slower or no faster and removed)

@@ -138,8 +138,8 @@ class Engine {
     bool tables_dirty_ = true;
     bool use_graph_ = true;
     bool full18_ = false;
-    // launch shape of the inner phases (engine.cu): one RHS per thread, 6 blocks per SM
-    // FP16: packed two-solve P1..P3 (fastest measured); FP32: one solve per thread
+    // launch shape of the inner phases (engine.cu) when the tuner has none: FP16 packed
+    // two-solve P1 / P3 (fastest measured at 32^4); FP32 one solve per thread
     int default_variant() const { return low_ == LOW_F16 ? 7 : 2; }
 };
 
