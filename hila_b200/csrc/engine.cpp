@@ -450,12 +450,14 @@ int Engine::launch_chunk(int iters) {
     int cls = 0, shape = -1, dyn = 1;
     want_variant_ = 0;
     if (const char *env = std::getenv("HW_ENGINE_SCHED")) dyn = std::atoi(env) != 0;
-    if (nshapes > 1 && (cls = work_class()) > 0) {
+    if (nshapes > 1 && (cls = work_class()) >= kTuneMinClass) {
         TuneEntry &e = tune_[cls];
         shape = e.chosen >= 0 ? e.chosen : e.next;
         want_variant_ = shapes[shape].variant;
         dyn = shapes[shape].dyn;
         if (e.chosen >= 0 || ctx_->engine_profile) cls = 0;  // decided, or profiling: no timing
+    } else {
+        cls = 0;
     }
     if (tables_.dyn != dyn) {
         tables_.dyn = dyn;
@@ -519,7 +521,24 @@ void Engine::tune_collect() {
     int running = 0;
     for (int j = 0; j < kEngMaxProb; j++) running += slots_[j].used && host_states_[j].status == ENG_RUNNING;
     TuneEntry &e = tune_[cls];
-    if (running != tune_pending_.running) return;  // the next chunk times the same candidate
+    const TuneShape *shapes = nullptr;
+    const int ns = tune_shapes(&shapes);
+    if (ns <= 0) return;
+    e.attempts++;
+    // after kTuneAttempts timed chunks per candidate, decide on the samples there are (a
+    // stream whose solves keep finishing inside chunks yields few countable ones)
+    auto decide = [&](bool complete) {
+        int best = -1;
+        for (int c = 0; c < ns; c++) {
+            if (complete && e.samples[c] < kTuneSamples) return;
+            if (e.samples[c] > 0 && (best < 0 || e.ms[c] < e.ms[best])) best = c;
+        }
+        e.chosen = best < 0 ? 0 : best;
+    };
+    if (running != tune_pending_.running) {  // the next chunk times the same candidate
+        if (e.attempts >= kTuneAttempts * ns) decide(false);
+        return;
+    }
     std::vector<double> it(n);
     for (int k = 0; k < n; k++) {
         const cudaEvent_t *ev = &tune_ev_[(size_t)k * (kEngPhases + 1)];
@@ -535,16 +554,9 @@ void Engine::tune_collect() {
     const double med = it[n / 2];
     if (e.samples[shape] == 0 || med < e.ms[shape]) e.ms[shape] = med;
     e.samples[shape]++;
-    const TuneShape *shapes = nullptr;
-    const int ns = tune_shapes(&shapes);
-    if (ns <= 0) return;
     e.next = (shape + 1) % ns;
-    int best = 0;
-    for (int c = 0; c < ns; c++) {
-        if (e.samples[c] < kTuneSamples) return;
-        if (e.ms[c] < e.ms[best]) best = c;
-    }
-    e.chosen = best;
+    decide(true);
+    if (e.chosen < 0 && e.attempts >= kTuneAttempts * ns) decide(false);
 }
 
 // Host-loop chunk with events around every phase; synchronises after each

@@ -33,13 +33,17 @@ struct TuneShape {
     int dyn;      // EngTables::dyn
 };
 constexpr int kTuneMaxShapes = 4;
-constexpr int kTuneSamples = 2;   // timed chunks per candidate
-constexpr int kTuneMaxIters = 16;  // iterations of a chunk with events
+constexpr int kTuneSamples = 2;     // timed chunks per candidate
+constexpr int kTuneMaxIters = 16;   // iterations of a chunk with events
+constexpr int kTuneMinClass = 10;   // smaller batches (< 512 tile-solves, about one wave of
+                                    // blocks) run the default shape untimed
+constexpr int kTuneAttempts = 4;    // timed chunks per candidate before deciding on what was seen
 struct TuneEntry {
     double ms[kTuneMaxShapes] = {};  // lowest median per-iteration time seen
     int samples[kTuneMaxShapes] = {};
-    int next = 0;     // candidate of the next timed chunk
-    int chosen = -1;  // index of the fastest, once every candidate has its samples
+    int attempts = 0;  // timed chunks, counted or not
+    int next = 0;      // candidate of the next timed chunk
+    int chosen = -1;   // index of the fastest, once every candidate has its samples
 };
 
 class Engine {

@@ -315,6 +315,10 @@ int admit_waiting(hw_server *S) {
         const size_t need = (size_t)q->nrhs * E.slot_bytes(l);
         if (S->bytes_in_use + need > S->cfg.hbm_budget_bytes) break;
         it = S->queue.erase(it);
+        // running from here on, so a failure below (fail_all) releases its slots and
+        // completes it instead of leaving its waiter behind
+        q->state = REQ_RUNNING;
+        S->running.push_back(q);
         q->bytes = need;
         S->bytes_in_use += need;
         q->t_admit = Clock::now();
@@ -358,8 +362,6 @@ int admit_waiting(hw_server *S) {
         }
         S->release_stage(*q);  // its conversions are enqueued: the entries can take new copies
         q->release_sources();
-        q->state = REQ_RUNNING;
-        S->running.push_back(q);
         admitted = true;
     }
     if (admitted) {  // the next chunk starts after the new sources are in place
@@ -515,6 +517,7 @@ void fail_all(hw_server *S, int rc) {
     S->worker_error = hw_last_error();
     for (auto &q : S->running) {
         for (int slot : q->slots) S->eng->release(slot);
+        S->release_stage(*q);
         q->release_solutions();  // possibly not copied: nothing is handed out
         q->res.status = rc;
         q->state = REQ_DONE;

@@ -448,7 +448,8 @@ int hw_engine_profile_get(hw_context *ctx, int precision, hw_engine_profile *out
  * order.  An engine times them on chunks of real iterations of the running solves
  * (median device time per iteration of P1..P4 and P5) and keeps the fastest per work
  * class, the bit length of the sum over the running Wilson solves of their lattice's
- * 128-site tiles.  A solve's result does not depend on the shape.  HW_ENGINE_TUNE=0
+ * 128-site tiles (classes below 10, about one wave of blocks, run the default shape
+ * untimed).  A solve's result does not depend on the shape.  HW_ENGINE_TUNE=0
  * turns the tuner off; HW_ENGINE_VARIANT or HW_ENGINE_SCHED force a shape instead. */
 #define HW_TUNE_MAX_SHAPES 4
 typedef struct hw_engine_tuning {
