@@ -433,12 +433,7 @@ int Engine::work_class() const {
         const EngLattice &L = tables_.lat[slots_[j].lat];
         if (L.fermion == FERM_WILSON) units += (unsigned long long)L.ntiles;
     }
-    int bits = 0;
-    while (units) {
-        bits++;
-        units >>= 1;
-    }
-    return bits;
+    return tune_work_class(units);
 }
 
 int Engine::launch_chunk(int iters) {
@@ -451,11 +446,11 @@ int Engine::launch_chunk(int iters) {
     want_variant_ = 0;
     if (const char *env = std::getenv("HW_ENGINE_SCHED")) dyn = std::atoi(env) != 0;
     if (nshapes > 1 && (cls = work_class()) >= kTuneMinClass) {
-        TuneEntry &e = tune_[cls];
-        shape = e.chosen >= 0 ? e.chosen : e.next;
+        bool timed = false;
+        shape = tune_pick(tune_[cls], &timed);
         want_variant_ = shapes[shape].variant;
         dyn = shapes[shape].dyn;
-        if (e.chosen >= 0 || ctx_->engine_profile) cls = 0;  // decided, or profiling: no timing
+        if (!timed || ctx_->engine_profile) cls = 0;  // decided, or profiling: no timing
     } else {
         cls = 0;
     }
@@ -520,23 +515,12 @@ void Engine::tune_collect() {
     if (cls <= 0 || n <= 0) return;
     int running = 0;
     for (int j = 0; j < kEngMaxProb; j++) running += slots_[j].used && host_states_[j].status == ENG_RUNNING;
-    TuneEntry &e = tune_[cls];
     const TuneShape *shapes = nullptr;
     const int ns = tune_shapes(&shapes);
     if (ns <= 0) return;
-    e.attempts++;
-    // after kTuneAttempts timed chunks per candidate, decide on the samples there are (a
-    // stream whose solves keep finishing inside chunks yields few countable ones)
-    auto decide = [&](bool complete) {
-        int best = -1;
-        for (int c = 0; c < ns; c++) {
-            if (complete && e.samples[c] < kTuneSamples) return;
-            if (e.samples[c] > 0 && (best < 0 || e.ms[c] < e.ms[best])) best = c;
-        }
-        e.chosen = best < 0 ? 0 : best;
-    };
-    if (running != tune_pending_.running) {  // the next chunk times the same candidate
-        if (e.attempts >= kTuneAttempts * ns) decide(false);
+    TuneEntry &e = tune_[cls];
+    if (running != tune_pending_.running) {  // a solve finished inside the chunk
+        tune_record(e, shape, ns, false, 0.0);
         return;
     }
     std::vector<double> it(n);
@@ -546,17 +530,13 @@ void Engine::tune_collect() {
         if (cudaEventElapsedTime(&a, ev[0], ev[PH_R1]) != cudaSuccess ||
             cudaEventElapsedTime(&b, ev[PH_P5], ev[kEngPhases]) != cudaSuccess) {
             cudaGetLastError();
+            tune_record(e, shape, ns, false, 0.0);
             return;
         }
         it[k] = (double)a + (double)b;
     }
     std::sort(it.begin(), it.end());
-    const double med = it[n / 2];
-    if (e.samples[shape] == 0 || med < e.ms[shape]) e.ms[shape] = med;
-    e.samples[shape]++;
-    e.next = (shape + 1) % ns;
-    decide(true);
-    if (e.chosen < 0 && e.attempts >= kTuneAttempts * ns) decide(false);
+    tune_record(e, shape, ns, true, it[n / 2]);
 }
 
 // Host-loop chunk with events around every phase; synchronises after each

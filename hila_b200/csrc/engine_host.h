@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "engine_tune.h"
 #include "hw_internal.h"
 
 namespace hw {
@@ -22,29 +23,10 @@ struct SlotInfo {
     int lat = -1;
 };
 
-// Online choice of the inner phases' launch shape.  The candidates round every product
-// and sum alike (the packed two-solve hop and the one-solve-per-thread hop, each with
-// the dynamic or the static tile order), so a solve's bits do not depend on the choice.
-// Each is timed on real iterations of the running batch (median over a chunk of the
-// device time of P1..P4 and P5, which the shape changes; the reliable-update phases do
-// not depend on it) and the fastest is kept per work class.
-struct TuneShape {
-    int variant;  // EngGrid::variant
-    int dyn;      // EngTables::dyn
-};
-constexpr int kTuneMaxShapes = 4;
-constexpr int kTuneSamples = 2;     // timed chunks per candidate
-constexpr int kTuneMaxIters = 16;   // iterations of a chunk with events
-constexpr int kTuneMinClass = 10;   // smaller batches (< 512 tile-solves, about one wave of
-                                    // blocks) run the default shape untimed
-constexpr int kTuneAttempts = 4;    // timed chunks per candidate before deciding on what was seen
-struct TuneEntry {
-    double ms[kTuneMaxShapes] = {};  // lowest median per-iteration time seen
-    int samples[kTuneMaxShapes] = {};
-    int attempts = 0;  // timed chunks, counted or not
-    int next = 0;      // candidate of the next timed chunk
-    int chosen = -1;   // index of the fastest, once every candidate has its samples
-};
+// Online choice of the inner phases' launch shape: the candidates (engine_tune.h) are
+// timed on real iterations of the running batch (median over a chunk of the device time
+// of P1..P4 and P5, which the shape changes; the reliable-update phases do not depend on
+// it) and the fastest is kept per work class.
 
 class Engine {
   public:
