@@ -594,10 +594,23 @@ __global__ void __launch_bounds__(kEngTile, 3) k_eng_f64(EngPtrs P) {
             epi_f64<PHASE, LOW>(pr, stride, i, acc, red);
         }
         if constexpr (NRED > 0) {
+            // the item's sums with one barrier: warp sums in shared memory, added by thread 0
+            // in warp order (block_sum's order, the same bits)
+            __shared__ double s_w[NRED][kEngTile / 32];
 #pragma unroll
             for (int k = 0; k < NRED; k++) {
-                double sum = block_sum<kEngTile>(red[k], smem);
-                if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
+                const double v = warp_sum(red[k]);
+                if ((threadIdx.x & 31) == 0) s_w[k][threadIdx.x >> 5] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int k = 0; k < NRED; k++) {
+                    double sum = 0;
+#pragma unroll
+                    for (int w = 0; w < kEngTile / 32; w++) sum += s_w[k][w];
+                    P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
+                }
             }
             arrive_and_finish<PHASE, NRED>(P, La, l, smem, last, La.ntiles * na);
         }
