@@ -62,6 +62,11 @@ WORKLOADS = {
     "serve32": dict(dims=(32, 32, 32, 32), eps=0.3, kappa=0.124, tol=1e-10, link_seed=100, src_seed=101,
                     lattices=[(32, 32, 32, 32)], requests=32, rate=10.0, kappa_range=(0.124, 0.124),
                     nrhs_range=(12, 12), pool=12),
+    # staggered fermions (dirac_staggered_evenodd) on the batched engine: 12 sources of M x = b
+    # solved together with FP16 inner iterations, against the same batch in FP64; the mass sits
+    # just above the hop's spectral radius (about 2.25 for these links), where M = m - D^dag D / m
+    # is still positive and hardest to solve
+    "stag": dict(dims=(32, 32, 32, 32), eps=0.3, mass=2.3, tol=1e-10, link_seed=100, src_seed=101, nrhs=12),
 }
 # CG iterations of one solve of each workload (FP64 CG on M^dag M, true residual 1e-10), used to turn the
 # reference arm's per-iteration time into solves/s.  Measured by the FP64 GPU CG on exactly these seeded
@@ -784,6 +789,84 @@ def serve_measure(ctx, w, args, rank: int = 0) -> dict:
     }
 
 
+def run_stag(args, dist: Dist):
+    """The staggered workload: a batch of staggered solves of M x = b on the engine with FP16
+    inner iterations and FP64 reliable updates (value), the same batch in FP64 on the engine,
+    and the standalone FP64 CG (CG<dirac_staggered_evenodd>, normal equations) for context."""
+    import torch
+    import hila_b200 as hw
+    torch.cuda.set_device(dist.local_rank)
+    dist.init("nccl")
+    w = WORKLOADS["stag"]
+    dims, nrhs = w["dims"], w["nrhs"]
+    ctx = hw.Context(dist.local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    lat = hw.Lattice(ctx, dims, True)
+    G = hw.GaugeField(lat, hw.generate_links(dims, w["eps"], w["link_seed"]), args.link_format)
+    D = hw.dirac_staggered_evenodd(w["mass"], G)
+    # seeded Gaussian colour vectors on the EVEN sites (spin component 0 of the spinor generator)
+    srcs = [np.ascontiguousarray(hw.generate_spinor(dims, w["src_seed"] + k, hw.EVEN)[:, 0]) for k in range(nrhs)]
+    fbs = [hw.StaggeredField(lat, v) for v in srcs]
+    fxs = [hw.StaggeredField(lat) for _ in srcs]
+
+    def batch(prec):
+        for f in fxs:
+            f.zero()
+        return hw.staggered_batch_solve(ctx, [(D, fb, fx, w["tol"]) for fb, fx in zip(fbs, fxs)], precision=prec,
+                                        delta=args.delta)
+
+    def timed(prec, steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        res = []
+        for _ in range(steps):
+            res += batch(prec)
+        ev1.record(stream)
+        ev1.synchronize()
+        return dist.max(ev0.elapsed_time(ev1) * 1e-3), res
+
+    for _ in range(args.warmup):
+        batch("f16")
+    batch("f64")
+    clocks = ClockSampler(dist.local_rank)
+    clocks.start()
+    t, res = timed("f16", args.steps)
+    clk = clocks.stop()
+    value = dist.world * args.steps * nrhs / t
+    t64, res64 = timed("f64", max(1, args.steps // 2))
+    fp64 = dist.world * max(1, args.steps // 2) * nrhs / t64
+    # the standalone FP64 CG on the normal equations of one source
+    fy = hw.StaggeredField(lat)
+    D.cg(fbs[0], fy, accuracy=w["tol"])
+    fy.zero()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    rcg = D.cg(fbs[0], fy, accuracy=w["tol"])
+    ev1.record(stream)
+    ev1.synchronize()
+    cfg = workload_config(args, dict(w, kappa=None), dist.world)
+    cfg.pop("kappa", None)
+    cfg["mass"] = w["mass"]
+    out = {
+        "metric": "staggered CG solves/s at 1e-10 residual (FP16 inner + FP64 reliable updates vs FP64)",
+        "value": round(value, 4), "unit": "solves/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t / args.steps * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16+f64",
+        "data": "synthetic: seeded SU(3) links exp(i eps H), Gaussian sources", "config": cfg,
+        "iterations": max(r.iterations for r in res), "reliable_updates": max(r.reliable_updates for r in res),
+        "true_residual": max(r.true_residual for r in res), "all_converged": all(r.converged for r in res),
+        "fp64_engine_solves_per_s": round(fp64, 3), "fp64_engine_iterations": max(r.iterations for r in res64),
+        "fp64_engine_all_converged": all(r.converged for r in res64), "speedup_vs_fp64_engine": round(value / fp64, 3),
+        "fp64_cg_normal_equations": {"solves_per_s": round(1e3 / ev0.elapsed_time(ev1), 3),
+                                     "iterations": rcg.iterations, "converged": rcg.converged},
+        "clocks": clk, "impl": "ours"}
+    if dist.rank == 0:
+        print(json.dumps(out))
+    dist.close()
+
+
 def run_serve(args, dist: Dist):
     """Poisson request stream through the server, and the same stream through the FP64 CG (FIFO)."""
     import torch
@@ -829,6 +912,11 @@ def run_reference(args, dist: Dist):
     if args.workload.startswith("serve"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; its FP64 CG "
                           "is timed on the cg and mrhs workloads"}), flush=True)
+        return
+    if args.workload == "stag":
+        print(json.dumps({"impl": "reference", "unavailable": "the stag workload compares the engine's FP16 and FP64 "
+                          "staggered solves on the GPU; the reference's CPU CG is timed on the cg and mrhs "
+                          "workloads"}), flush=True)
         return
     if args.workload == "dslash":
         samples = [cpu_sample("cg", seconds_budget=2.0) for _ in range(args.warmup + args.steps)][args.warmup:]
@@ -899,6 +987,7 @@ def main():
     ap.add_argument("--nrhs", type=int, default=None, help="override the right-hand sides per step (mrhs)")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=None, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--mass", type=float, default=None, help="stag: staggered mass")
     args = ap.parse_args()
     if args.precision is None:
         args.precision = "f16" if args.workload in ("mrhs", "serve", "serve32") else "f64"
@@ -912,6 +1001,8 @@ def main():
         WORKLOADS[args.workload]["dims"] = tuple(int(v) for v in args.lattice.split("x"))
     if args.nrhs:
         WORKLOADS[args.workload]["nrhs"] = args.nrhs
+    if args.mass and args.workload == "stag":
+        WORKLOADS["stag"]["mass"] = args.mass
     if args.no_graph:
         os.environ["HW_USE_GRAPH"] = "0"
     if args.warmup < 3:
@@ -921,6 +1012,8 @@ def main():
         run_reference(args, dist)
     elif args.workload.startswith("serve"):
         run_serve(args, dist)
+    elif args.workload == "stag":
+        run_stag(args, dist)
     else:
         run_ours(args, dist)
 

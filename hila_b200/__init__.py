@@ -115,7 +115,7 @@ class _SolveRequest(ctypes.Structure):
 class _StagSolveRequest(ctypes.Structure):
     _fields_ = [("gauge", ctypes.c_void_p), ("mass", ctypes.c_double), ("inp", ctypes.c_void_p),
                 ("out", ctypes.c_void_p), ("accuracy", ctypes.c_double), ("maxiters", ctypes.c_int),
-                ("normal", ctypes.c_int)]
+                ("normal", ctypes.c_int), ("precision", ctypes.c_int), ("delta", ctypes.c_double)]
 
 
 _vp = ctypes.c_void_p
@@ -157,6 +157,7 @@ _SIGNATURES = {
     "hw_stag_field_destroy": (ctypes.c_int, [_vp]),
     "hw_stag_field_upload": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "hw_stag_field_download": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+    "hw_stag_field_zero": (ctypes.c_int, [_vp, ctypes.c_int]),
     "hw_staggered_evenodd_apply": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_staggered_evenodd_dagger": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp]),
     "hw_staggered_evenodd_force": (ctypes.c_int, [_vp, ctypes.c_double, _vp, _vp, ctypes.c_int, _dp]),
@@ -571,6 +572,9 @@ class StaggeredField:
         _check(lib().hw_stag_field_download(self.handle, _dptr(out), int(parity)))
         return out
 
+    def zero(self, parity: int = ALL):
+        _check(lib().hw_stag_field_zero(self.handle, int(parity)))
+
     def close(self):
         if self.handle:
             lib().hw_stag_field_destroy(self.handle)
@@ -772,10 +776,14 @@ def batch_solve(ctx: Context, requests, precision: str = "f16", delta: float = 0
     return [CGResult.from_c(res[k]) for k in range(n)]
 
 
-def staggered_batch_solve(ctx: Context, requests) -> list:
+def staggered_batch_solve(ctx: Context, requests, precision: str = "f64", delta: float = 0.0) -> list:
     """Many staggered solves at once on the batched engine (hw_staggered_batch_solve):
     requests are (dirac_staggered_evenodd, in_field, out_field[, accuracy[, maxiters[, normal]]]);
-    normal=False solves M out = in, normal=True M^dag M out = in (CG<Op>::apply)."""
+    normal=False solves M out = in, normal=True M^dag M out = in (CG<Op>::apply).
+    precision "f64" runs FP64 throughout, "f16" the inner iterations on FP16 fields with
+    FP64 reliable updates (delta <= 0: 0.005)."""
+    if precision not in ("f64", "f16"):
+        raise ValueError("staggered precision is 'f64' or 'f16'")
     n = len(requests)
     arr = (_StagSolveRequest * max(n, 1))()
     for k, req in enumerate(requests):
@@ -784,7 +792,7 @@ def staggered_batch_solve(ctx: Context, requests) -> list:
         mi = req[4] if len(req) > 4 else 10000
         normal = req[5] if len(req) > 5 else False
         arr[k] = _StagSolveRequest(op.gauge.handle.value, op.mass, b.handle.value, x.handle.value, float(acc),
-                                   int(mi), int(bool(normal)))
+                                   int(mi), int(bool(normal)), PRECISIONS[precision], float(delta))
     res = (_CgResult * max(n, 1))()
     rc = lib().hw_staggered_batch_solve(ctx.handle, arr, n, res)
     if rc not in (HW_OK, HW_ERR_NOT_CONVERGED, HW_ERR_BREAKDOWN):

@@ -264,6 +264,15 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
         }
     HW_CHECK_ARG(slot >= 0, "no free solve slot (%d in use)", kEngMaxProb);
     int rc;
+    // a staggered solve with a reliable-update factor runs its inner iterations in FP16
+    // (engine_stag.cuh), which reads the 18-real FP16 links
+    const bool stag_low = L.fermion == FERM_STAGGERED && delta > 0.0;
+    if (stag_low) {
+        HW_CHECK_ARG(low_ == LOW_F16 && full18_, "low-precision staggered solves need the FP16 engine with 18-real links");
+        if ((rc = ensure_low_links(gauges_[lat], low_, full18_)) != HW_OK) return rc;
+        L.l16x = gauges_[lat]->f16x.as<uint4>();
+        L.l16z = gauges_[lat]->f16z.as<unsigned>();
+    }
     if ((rc = ensure_slot_buffers(slot, L.stride)) != HW_OK) return rc;
     SlotBuffers &B = bufs_[slot];
     if (!b || !x) {
@@ -275,6 +284,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     std::memset(&P, 0, sizeof(P));
     P.lat = lat;
     P.mode = mode;
+    P.stag_low = stag_low ? 1 : 0;
     P.kappa = kappa;
     P.diag = diag;
     P.p = B.p.ptr;

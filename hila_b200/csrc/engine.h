@@ -44,6 +44,9 @@ enum EngStatus : int { ENG_RUNNING = 0, ENG_CONVERGED = 1, ENG_MAXITER = 2, ENG_
 //   P4 r -= alpha (m Dp + D^{eo}_- t), x += alpha p (FP64), |r|^2
 //   R1 flags a nonzero initial x; R2, R3 s = b - M x; R4(L), R5(L) r = M^dag s; P5 p = r + beta p
 // with D_s = 0.5 s hop (staggered.h:48-68) and the slot's kappa holding the mass m.
+// A slot with stag_low set runs P1..P5 in FP32 arithmetic on FP16 fields with a per-site
+// norm and FP16 links, P4 accumulating alpha p in the FP32 y, R1 x += y, and the reliable
+// update in FP64 (t64 holds the odd FP64 half, R5(L) stores r in FP16).
 enum EngFermion : int { FERM_WILSON = 0, FERM_STAGGERED = 1 };
 enum EngMode : int { ENG_MODE_SOLVE = 0, ENG_MODE_NORMAL = 1 };
 
@@ -70,6 +73,8 @@ struct EngLattice {
 struct EngProblem {
     int lat;
     int mode;
+    int stag_low;  // staggered slot with FP16 inner iterations (FP64 reliable updates); 0: FP64 throughout
+    int pad;
     double kappa;
     double diag;  // 1 + m_h: the Hasenbusch operator M + m_h (Hasenbusch.h:16-52); 1 for M
     // low precision (EVEN: p, r, Dp; ODD: t); FP16 fields carry a norm plane

@@ -13,6 +13,143 @@
 // staggered_math.cuh, which engine.cu includes at file scope.
 #pragma once
 
+// An FP16 colour-vector half lattice of a low-precision staggered slot: the three
+// colours as (re, im) half pairs in the first uint4 plane of the slot's buffer (the
+// fourth word unused) and a per-site scale, the largest |component| of the site.
+struct HalfStag16 {
+    uint4 *p;
+    float *n;
+    __device__ __forceinline__ static void unpack(uint4 v, float s, Cx<float> w[3]) {
+        const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 f = __half22float2(h[c]);
+            w[c] = {f.x * s, f.y * s};
+        }
+    }
+    __device__ __forceinline__ void ld(int i, Cx<float> w[3]) const { unpack(__ldg(p + i), __ldg(n + i), w); }
+    // plain (coherent) load, for arrays the same kernel also writes
+    __device__ __forceinline__ void ldp(int i, Cx<float> w[3]) const { unpack(p[i], n[i], w); }
+    __device__ __forceinline__ void st(int i, const Cx<float> w[3]) const {
+        float m = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf(w[c].re), fabsf(w[c].im)));
+        const float inv = m > 0.f ? 1.0f / m : 0.f;
+        n[i] = m;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h[c] = __floats2half2_rn(w[c].re * inv, w[c].im * inv);
+        p[i] = v;
+    }
+};
+
+// The FP32 solution increment y of a low-precision staggered slot: colour c of site i at
+// y[c * stride + i] (the slot's y buffer viewed as float2 planes).
+struct HalfStagY {
+    float2 *p;
+    int stride;
+    __device__ __forceinline__ Cx<float> ld(int c, int i) const {
+        const float2 v = p[(size_t)c * stride + i];
+        return {v.x, v.y};
+    }
+    __device__ __forceinline__ void st(int c, int i, Cx<float> v) const {
+        p[(size_t)c * stride + i] = make_float2(v.re, v.im);
+    }
+};
+
+// stag_hop_site in FP32 from FP16 fields and the 18-real FP16 links
+__device__ __forceinline__ void stag_hop_site_low(const Geom &g, const LinksF16x18 &U, int par, int i,
+                                                  const HalfStag16 &v, Cx<float> acc[3]) {
+    const SiteNbrs n = site_neighbours(g, i, par);
+    int c[4];
+    site_coords(g, i, par, c);
+#pragma unroll
+    for (int a = 0; a < 3; a++) acc[a] = {0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const float eta = (float)stag_eta(c, d);
+        const float sf = (d == 3 && n.tfwd_wrap) ? -eta : eta;
+        const float sb = (d == 3 && n.tbwd_wrap) ? -eta : eta;
+        Su3<float> u;
+        Cx<float> w[3];
+        U.load(par, d, i, u);
+        v.ld(n.fwd[d], w);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const Cx<float> t = cmul(u.e[a][0], w[0]) + cmul(u.e[a][1], w[1]) + cmul(u.e[a][2], w[2]);
+            acc[a] = acc[a] + sf * t;
+        }
+        U.load(1 - par, d, n.bwd[d], u);
+        v.ld(n.bwd[d], w);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const Cx<float> t = cmul(conj(u.e[0][a]), w[0]) + cmul(conj(u.e[1][a]), w[1]) + cmul(conj(u.e[2][a]), w[2]);
+            acc[a] = acc[a] - sb * t;
+        }
+    }
+}
+
+// P1..P5 of a low-precision staggered slot at site i (FP32 arithmetic, FP16 fields);
+// red[0] receives the phase's |.|^2 contribution
+template <int PHASE>
+__device__ __forceinline__ void stag_low_site(const EngLattice &La, const EngProblem &pr, const EngState &st,
+                                              int i, double *red) {
+    constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2) ? 1 : -1;
+    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3) ? 1 : 0;
+    const int stride = La.stride;
+    const float m = (float)pr.kappa;  // the mass
+    const HalfStag16 p{static_cast<uint4 *>(pr.p), pr.pn}, r{static_cast<uint4 *>(pr.r), pr.rn};
+    const HalfStag16 Dp{static_cast<uint4 *>(pr.Dp), pr.Dpn}, t{static_cast<uint4 *>(pr.t), pr.tn};
+    if constexpr (PHASE == PH_P5) {
+        Cx<float> rv[3], pv[3];
+        r.ld(i, rv);
+        if (!st.init) {
+            const float beta = (float)st.beta;
+            p.ldp(i, pv);
+#pragma unroll
+            for (int c = 0; c < 3; c++) rv[c] = rv[c] + beta * pv[c];
+        }
+        p.st(i, rv);
+    } else {
+        const HalfStag16 in = PHASE == PH_P1 ? p : PHASE == PH_P3 ? Dp : t;
+        Cx<float> acc[3], h[3];
+        stag_hop_site_low(La.g, LinksF16x18{La.l16x, La.l16z, stride}, OUTPAR, i, in, acc);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h[c] = (0.5f * SIGN) * acc[c];
+        if constexpr (OUTPAR == 1) {  // P1, P3: t = (1/m) D in
+            const float im = 1.0f / m;
+#pragma unroll
+            for (int c = 0; c < 3; c++) h[c] = im * h[c];
+            t.st(i, h);
+        } else if constexpr (PHASE == PH_P2) {  // Dp = m p + D t
+            Cx<float> pv[3];
+            p.ld(i, pv);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                h[c] = m * pv[c] + h[c];
+                red[0] += (double)norm2(h[c]);
+            }
+            Dp.st(i, h);
+        } else {  // P4: r -= alpha (m Dp + D t), y += alpha p
+            const float alpha = (float)st.alpha;
+            Cx<float> dv[3], rv[3], pv[3];
+            Dp.ld(i, dv);
+            r.ldp(i, rv);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                rv[c] = rv[c] - alpha * (m * dv[c] + h[c]);
+                red[0] += (double)norm2(rv[c]);
+            }
+            r.st(i, rv);
+            p.ld(i, pv);
+            const HalfStagY y{reinterpret_cast<float2 *>(pr.y), stride};
+#pragma unroll
+            for (int c = 0; c < 3; c++) y.st(c, i, y.ld(c, i) + alpha * pv[c]);
+        }
+    }
+}
+
 template <int PHASE>
 __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
     constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2 || PHASE == PH_R2 || PHASE == PH_R3) ? 1 : -1;
@@ -44,11 +181,17 @@ __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
         const EngProblem &pr = T->prob[j];
         const EngState &st = P.S[j];
         const double m = pr.kappa;  // the mass of a staggered solve
+        const bool low = pr.stag_low != 0;
         const HalfStag x{pr.x, stride}, b{pr.b, stride}, sv{pr.s, stride};
         const HalfStag p{static_cast<double2 *>(pr.p), stride}, r{static_cast<double2 *>(pr.r), stride};
-        const HalfStag Dp{static_cast<double2 *>(pr.Dp), stride}, t{static_cast<double2 *>(pr.t), stride};
+        const HalfStag Dp{static_cast<double2 *>(pr.Dp), stride};
+        // the odd FP64 half of the reliable update: t itself, or t64 beside the FP16 t
+        const HalfStag t{low ? pr.t64 : static_cast<double2 *>(pr.t), stride};
         double red[2] = {0.0, 0.0};
-        if (i < g.Vh) {
+        constexpr bool INNER = PHASE == PH_P1 || PHASE == PH_P2 || PHASE == PH_P3 || PHASE == PH_P4 || PHASE == PH_P5;
+        if (i < g.Vh && INNER && low) {
+            stag_low_site<PHASE>(La, pr, st, i, red);
+        } else if (i < g.Vh) {
             if constexpr (PHASE == PH_R1) {
                 // first update: record whether the initial x is nonzero anywhere (read by R2, R3)
                 bool nz = false;
@@ -61,6 +204,16 @@ __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
                 if (st.init && __any_sync(am, nz) && (threadIdx.x & 31) == __ffs(am) - 1 &&
                     !*(volatile int *)&P.S[j].xnz)
                     atomicOr(&P.S[j].xnz, 1);
+                if (low) {  // x += y, y = 0
+                    const HalfStagY y{reinterpret_cast<float2 *>(pr.y), stride};
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const Cx<float> yv = y.ld(c, i);
+                        const Cx<double> xv = x.ldp(c, i);
+                        x.st(c, i, {xv.re + (double)yv.re, xv.im + (double)yv.im});
+                        y.st(c, i, {0.f, 0.f});
+                    }
+                }
             } else if constexpr (PHASE == PH_P5) {
                 const double beta = st.beta;
 #pragma unroll
@@ -120,30 +273,46 @@ __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
                             sv.st(c, i, mx);
                         }
                     }
-                } else if constexpr (PHASE == PH_R5L) {  // r = M^dag s
+                } else if constexpr (PHASE == PH_R5L || PHASE == PH_R5) {
+                    // R5L: r = M^dag s; R5: r = b - M^dag M x (normal system); FP16 r for a
+                    // low-precision slot
+                    Cx<float> rl[3];
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
-                        const Cx<double> v = m * sv.ld(c, i) + h[c];
-                        r.st(c, i, v);
+                        Cx<double> v = m * sv.ld(c, i) + h[c];
+                        if (PHASE == PH_R5) {
+                            const Cx<double> bv = b.ld(c, i);
+                            v = bv - v;
+                            red[1] += norm2(bv);
+                        }
                         red[0] += norm2(v);
+                        if (low)
+                            rl[c] = {(float)v.re, (float)v.im};
+                        else
+                            r.st(c, i, v);
                     }
-                } else if constexpr (PHASE == PH_R5) {  // r = b - M^dag M x
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const Cx<double> bv = b.ld(c, i);
-                        const Cx<double> v = bv - (m * sv.ld(c, i) + h[c]);
-                        r.st(c, i, v);
-                        red[0] += norm2(v);
-                        red[1] += norm2(bv);
-                    }
+                    if (low) HalfStag16{static_cast<uint4 *>(pr.r), pr.rn}.st(i, rl);
                 }
             }
         }
         if constexpr (NRED > 0) {
+            // the item's sums with one barrier: warp sums in shared memory, added by thread 0
+            // in warp order (block_sum's order, the same bits)
+            __shared__ double s_w[NRED][kEngTile / 32];
 #pragma unroll
             for (int k = 0; k < NRED; k++) {
-                const double sum = block_sum<kEngTile>(red[k], smem);
-                if (threadIdx.x == 0) P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
+                const double v = warp_sum(red[k]);
+                if ((threadIdx.x & 31) == 0) s_w[k][threadIdx.x >> 5] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int k = 0; k < NRED; k++) {
+                    double sum = 0;
+#pragma unroll
+                    for (int w = 0; w < kEngTile / 32; w++) sum += s_w[k][w];
+                    P.partials[((size_t)j * 2 + k) * max_tiles + lt] = sum;
+                }
             }
             arrive_and_finish<PHASE, NRED, FERM_STAGGERED>(P, La, l, smem, last, La.ntiles * na);
         }

@@ -193,10 +193,12 @@ int hw_staggered_batch_solve(hw_context *ctx, const hw_stag_solve_request *reqs,
         HW_CHECK_ARG(q.in != q.out, "request %d: in and out must differ", k);
         HW_CHECK_ARG(q.accuracy > 0 && q.maxiters > 0, "request %d: bad accuracy or maxiters", k);
         HW_CHECK_ARG(std::isfinite(q.mass) && q.mass != 0.0, "request %d: mass must be finite and nonzero", k);
+        HW_CHECK_ARG(q.precision == HW_PREC_F64 || q.precision == HW_PREC_F16,
+                     "request %d: staggered precision must be HW_PREC_F64 or HW_PREC_F16", k);
     }
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     HW_CUDA(cudaSetDevice(ctx->device));
-    // staggered slots run their own FP64 phases in the engine that also serves FP16 Wilson solves
+    // staggered slots run their own phases in the engine that also serves FP16 Wilson solves
     Engine *E;
     int rc;
     if ((rc = get_engine(ctx, LOW_F16, &E)) != HW_OK) return rc;
@@ -207,9 +209,11 @@ int hw_staggered_batch_solve(hw_context *ctx, const hw_stag_solve_request *reqs,
         [&](int k, int *l) { return E->lattice_index(reqs[k].gauge, l, FERM_STAGGERED); },
         [&](int k, int l, int *slot) {
             const hw_stag_solve_request &q = reqs[k];
-            // FP64 throughout: a reliable update only confirms convergence (delta 0)
+            // FP64 throughout: a reliable update only confirms convergence (delta 0); FP16
+            // inner iterations: a reliable update when |r| fell by delta
+            const double delta = q.precision == HW_PREC_F16 ? (q.delta > 0 ? q.delta : 0.005) : 0.0;
             return E->admit(l, q.mass, q.in->half[0].as<double2>(), q.out->half[0].as<double2>(), q.accuracy,
-                            q.maxiters, 0.0, q.normal ? ENG_MODE_NORMAL : ENG_MODE_SOLVE, slot);
+                            q.maxiters, delta, q.normal ? ENG_MODE_NORMAL : ENG_MODE_SOLVE, slot);
         },
         [&](int k) { return cudaMemsetAsync(reqs[k].out->half[1].ptr, 0, reqs[k].out->half[1].bytes, ctx->stream); });
 }

@@ -280,6 +280,18 @@ int hw_stag_field_download(const hw_stag_field *f, double *host, int parity) {
     return HW_OK;
 }
 
+int hw_stag_field_zero(hw_stag_field *f, int parity) {
+    HW_CHECK_ARG(f, "null argument");
+    HW_CHECK_ARG(parity >= 1 && parity <= 3, "parity must be HW_EVEN, HW_ODD or HW_ALL");
+    hw_context *ctx = f->lat->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    HW_CUDA(cudaSetDevice(ctx->device));
+    for (int p = 0; p < 2; p++)
+        if (parity & (1 << p)) HW_CUDA(cudaMemsetAsync(f->half[p].ptr, 0, f->half[p].bytes, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return HW_OK;
+}
+
 int hw_staggered_evenodd_apply(const hw_gauge *gauge, double mass, const hw_stag_field *in, hw_stag_field *out) {
     return stag_apply(gauge, mass, in, out, +1);
 }

@@ -374,6 +374,8 @@ int hw_stag_field_destroy(hw_stag_field *field);
 int hw_stag_field_upload(hw_stag_field *field, const double *host, int parity);
 /* sites of the parities not requested come back as zero */
 int hw_stag_field_download(const hw_stag_field *field, double *host, int parity);
+/* zero the sites of `parity` (the field's memory stays allocated) */
+int hw_stag_field_zero(hw_stag_field *field, int parity);
 
 /* dirac_staggered_evenodd<SU<3,double>>::apply / dagger, staggered.h:224-242:
  * out[EVEN] = m in_e + D_eo (1/m) D_oe in_e with D = 0.5 s sum_mu eta_mu (U fwd -
@@ -396,13 +398,17 @@ typedef struct hw_stag_solve_request {
     int normal;                /* 1: M^dag M out = in, CG<Op>::apply semantics (conjugate_gradient.h:46-104),
                                   residual |in - M^dag M out| / |in|; 0: M out = in, residual
                                   |in - M out| / |in| (CG on M^dag M with source M^dag in) */
+    int precision;             /* HW_PREC_F64 (0): FP64 throughout; HW_PREC_F16: inner iterations in
+                                  FP32 arithmetic on FP16 fields with FP64 reliable updates */
+    double delta;              /* HW_PREC_F16: reliable-update factor (<= 0: 0.005) */
 } hw_stag_solve_request;
 /* Many staggered solves on many lattices at once, on the same batched engine as the
  * Wilson solves (no reference counterpart: HILA runs one CG<Op>::apply per source):
- * FP64 CG in one kernel launch per phase for all admitted solves, up to 16 per lattice
- * and 64 in total at a time; results[k] is request k's outcome (iterations,
- * recomputed FP64 true residual); each solve gives bitwise the same result alone and
- * in any batch, also beside Wilson solves of the same engine. */
+ * CG in one kernel launch per phase for all admitted solves, up to 16 per lattice and
+ * 64 in total at a time, in FP64 or mixed precision per request (the FP64 solution, the
+ * reliable updates and the convergence test always in FP64); results[k] is request k's
+ * outcome (iterations, recomputed FP64 true residual); each solve gives bitwise the
+ * same result alone and in any batch, also beside Wilson solves of the same engine. */
 int hw_staggered_batch_solve(hw_context *ctx, const hw_stag_solve_request *requests, int n, hw_cg_result *results);
 /* CG<dirac_staggered_evenodd>::apply, conjugate_gradient.h:46-104: M^dag M out = in
  * on EVEN, out the initial guess; FP64 (params->precision must be HW_PREC_F64);

@@ -112,3 +112,38 @@ def test_staggered_and_wilson_in_one_server(hw, ctx, oracle):
             assert np.array_equal(a.download(), f.download())
     finally:
         srv.close()
+
+
+def test_staggered_batch_mixed_precision(hw, ctx, oracle):
+    """FP16 inner iterations with FP64 reliable updates (precision "f16"): masses from just
+    above the spectral radius of the hop (|D| is about 2.25 for these links, so at m = 2.4
+    M = m - D^dag D / m stays positive with a condition number near 8) to heavy, both link
+    formats, both systems; every solve reaches the oracle's FP64 true residual, the lightest
+    takes several reliable updates, and a solve is bitwise the same alone as in the batch."""
+    built = build(hw, ctx, oracle, [((8, 8, 8, 8), 331, 2.4, 3, 18), ((4, 4, 4, 8), 332, 4.5, 1, 12),
+                                     ((2, 4, 6, 8), 333, 6.0, 1, 18)])
+    work = []
+    for n, (dims, U, lat, G, D, mass, srcs) in enumerate(built):
+        for k, b in enumerate(srcs):
+            normal = (n, k) == (0, 2)
+            work.append((dims, U, lat, D, mass, b, normal, hw.StaggeredField(lat, b), hw.StaggeredField(lat)))
+    reqs = [(D, fb, fx, TOL, 10000, normal) for (_, _, _, D, _, _, normal, fb, fx) in work]
+    res = hw.staggered_batch_solve(ctx, reqs, precision="f16")
+    for (dims, U, lat, D, mass, b, normal, fb, fx), r in zip(work, res):
+        assert r.converged, r
+        x = fx.download()
+        assert residual(oracle, dims, U, mass, b, x, normal=normal) <= TOL
+        if mass < 3:
+            assert r.reliable_updates >= 2, r
+        alone = hw.StaggeredField(lat)
+        [ra] = hw.staggered_batch_solve(ctx, [(D, fb, alone, TOL, 10000, normal)], precision="f16")
+        assert ra.iterations == r.iterations
+        assert np.array_equal(alone.download(), x)
+    # the same light-mass system in FP64 on the engine: the same solution to the tolerance
+    (dims, U, lat, D, mass, b, normal, fb, fx) = work[0]
+    f64 = hw.StaggeredField(lat)
+    [r64] = hw.staggered_batch_solve(ctx, [(D, fb, f64, TOL)])
+    assert r64.converged
+    ev = oracle.parity_mask(dims) == 0
+    x, y = fx.download(), f64.download()
+    assert np.linalg.norm(_c(x)[ev] - _c(y)[ev]) / np.linalg.norm(_c(y)[ev]) <= 1e-6
