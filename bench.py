@@ -992,7 +992,7 @@ def main():
     if args.precision is None:
         args.precision = "f16" if args.workload in ("mrhs", "serve", "serve32") else "f64"
     if args.delta is None:
-        args.delta = 1e-5 if args.precision == "f32" else 0.005
+        args.delta = 1e-5 if args.precision == "f32" else (0.05 if args.workload == "stag" else 0.005)
     if args.requests and args.workload.startswith("serve"):
         WORKLOADS[args.workload]["requests"] = args.requests
     if args.rate and args.workload.startswith("serve"):

@@ -781,7 +781,7 @@ def staggered_batch_solve(ctx: Context, requests, precision: str = "f64", delta:
     requests are (dirac_staggered_evenodd, in_field, out_field[, accuracy[, maxiters[, normal]]]);
     normal=False solves M out = in, normal=True M^dag M out = in (CG<Op>::apply).
     precision "f64" runs FP64 throughout, "f16" the inner iterations on FP16 fields with
-    FP64 reliable updates (delta <= 0: 0.005)."""
+    FP64 reliable updates (delta <= 0: 0.05)."""
     if precision not in ("f64", "f16"):
         raise ValueError("staggered precision is 'f64' or 'f16'")
     n = len(requests)

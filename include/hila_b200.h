@@ -400,7 +400,7 @@ typedef struct hw_stag_solve_request {
                                   |in - M out| / |in| (CG on M^dag M with source M^dag in) */
     int precision;             /* HW_PREC_F64 (0): FP64 throughout; HW_PREC_F16: inner iterations in
                                   FP32 arithmetic on FP16 fields with FP64 reliable updates */
-    double delta;              /* HW_PREC_F16: reliable-update factor (<= 0: 0.005) */
+    double delta;              /* HW_PREC_F16: reliable-update factor (<= 0: 0.05) */
 } hw_stag_solve_request;
 /* Many staggered solves on many lattices at once, on the same batched engine as the
  * Wilson solves (no reference counterpart: HILA runs one CG<Op>::apply per source):
