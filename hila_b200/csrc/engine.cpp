@@ -309,7 +309,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     std::memset(&S, 0, sizeof(S));
     S.status = ENG_RUNNING;
     S.mode = mode;
-    S.fermion = L.fermion;
+    S.fermion = stag_low ? FERM_STAGGERED_LOW : L.fermion;
     S.ru = 1;
     S.init = 1;
     S.tol2 = tol * tol;

@@ -74,7 +74,11 @@ __device__ __forceinline__ int find_lattice(const EngTables *T, int tile) {
 // which run after every tile of the lattice is done, so all blocks agree.
 template <int PHASE, int FERM = FERM_WILSON>
 __device__ __forceinline__ bool active(const EngState &s) {
-    if (s.fermion != FERM) return false;  // the other fermion's kernels serve this slot
+    // the other fermion's kernels serve this slot; the FP64 staggered kernels also run the
+    // reliable update of the staggered slots with FP16 inner iterations
+    const bool mine = s.fermion == FERM ||
+                      (FERM == FERM_STAGGERED && s.fermion == FERM_STAGGERED_LOW && eng_ru_phase(PHASE));
+    if (!mine) return false;
     // the first update of a solve from x = 0: H x is zero, R2 has nothing to do
     if (PHASE == PH_R2) return s.ru != 0 && !(s.init && !s.xnz);
     if (PHASE == PH_R4 || PHASE == PH_R5) return s.ru != 0 && s.mode == ENG_MODE_NORMAL;

@@ -47,7 +47,9 @@ enum EngStatus : int { ENG_RUNNING = 0, ENG_CONVERGED = 1, ENG_MAXITER = 2, ENG_
 // A slot with stag_low set runs P1..P5 in FP32 arithmetic on FP16 fields with a per-site
 // norm and FP16 links, P4 accumulating alpha p in the FP32 y, R1 x += y, and the reliable
 // update in FP64 (t64 holds the odd FP64 half, R5(L) stores r in FP16).
-enum EngFermion : int { FERM_WILSON = 0, FERM_STAGGERED = 1 };
+// (a slot's EngState.fermion is FERM_STAGGERED_LOW for a staggered solve with FP16 inner
+// iterations; lattice entries are FERM_WILSON or FERM_STAGGERED)
+enum EngFermion : int { FERM_WILSON = 0, FERM_STAGGERED = 1, FERM_STAGGERED_LOW = 2 };
 enum EngMode : int { ENG_MODE_SOLVE = 0, ENG_MODE_NORMAL = 1 };
 
 struct EngLattice {

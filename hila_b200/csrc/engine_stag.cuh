@@ -58,10 +58,11 @@ struct HalfStagY {
     }
 };
 
-// stag_hop_site in FP32 from FP16 fields and the 18-real FP16 links
-__device__ __forceinline__ void stag_hop_site_low(const Geom &g, const LinksF16x18 &U, int par, int i,
+// stag_hop_site in FP32 from FP16 fields and 18-real FP16 links (from memory, or the
+// tile's copy in shared memory); n: the neighbours of site i of output parity par
+template <class Lk>
+__device__ __forceinline__ void stag_hop_site_low(const Geom &g, const Lk &U, const SiteNbrs &n, int par, int i,
                                                   const HalfStag16 &v, Cx<float> acc[3]) {
-    const SiteNbrs n = site_neighbours(g, i, par);
     int c[4];
     site_coords(g, i, par, c);
 #pragma unroll
@@ -92,9 +93,9 @@ __device__ __forceinline__ void stag_hop_site_low(const Geom &g, const LinksF16x
 
 // P1..P5 of a low-precision staggered slot at site i (FP32 arithmetic, FP16 fields);
 // red[0] receives the phase's |.|^2 contribution
-template <int PHASE>
+template <int PHASE, class Lk>
 __device__ __forceinline__ void stag_low_site(const EngLattice &La, const EngProblem &pr, const EngState &st,
-                                              int i, double *red) {
+                                              const Lk &U, const SiteNbrs &nb, int i, double *red) {
     constexpr int SIGN = (PHASE == PH_P1 || PHASE == PH_P2) ? 1 : -1;
     constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3) ? 1 : 0;
     const int stride = La.stride;
@@ -114,7 +115,7 @@ __device__ __forceinline__ void stag_low_site(const EngLattice &La, const EngPro
     } else {
         const HalfStag16 in = PHASE == PH_P1 ? p : PHASE == PH_P3 ? Dp : t;
         Cx<float> acc[3], h[3];
-        stag_hop_site_low(La.g, LinksF16x18{La.l16x, La.l16z, stride}, OUTPAR, i, in, acc);
+        stag_hop_site_low(La.g, U, nb, OUTPAR, i, in, acc);
 #pragma unroll
         for (int c = 0; c < 3; c++) h[c] = (0.5f * SIGN) * acc[c];
         if constexpr (OUTPAR == 1) {  // P1, P3: t = (1/m) D in
@@ -147,6 +148,85 @@ __device__ __forceinline__ void stag_low_site(const EngLattice &La, const EngPro
 #pragma unroll
             for (int c = 0; c < 3; c++) y.st(c, i, y.ld(c, i) + alpha * pv[c]);
         }
+    }
+}
+
+// P1..P5 of the staggered slots with FP16 inner iterations, in the shape of the Wilson
+// inner phases: a block walks tiles (block + k x grid); per tile, the sites' eight FP16
+// links are copied into shared memory once and read from there by every such slot of the
+// lattice, and each slot's partial sum is formed once per tile in block_sum's order.
+template <int PHASE>
+__global__ void __launch_bounds__(kEngTile, 4) k_stag_low(EngPtrs P) {
+    constexpr int OUTPAR = (PHASE == PH_P1 || PHASE == PH_P3) ? 1 : 0;
+    constexpr int NRED = (PHASE == PH_P2 || PHASE == PH_P4) ? 1 : 0;
+    constexpr bool HOP = PHASE != PH_P5;
+    __shared__ double smem[kEngTile / 32];
+    __shared__ bool last;
+    __shared__ int s_act[kEngMaxRhs];
+    __shared__ int s_na;
+    __shared__ uint4 s_lx[HOP ? 16 * kEngTile : 1];
+    __shared__ unsigned s_lz[HOP ? 8 * kEngTile : 1];
+    __shared__ double s_red[NRED > 0 ? kEngMaxRhs : 1][kEngTile / 32];
+    const EngTables *T = P.T;
+    const int ntiles = T->ntiles;
+    const int max_tiles = T->max_tiles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int l = find_lattice(T, tile);
+        const EngLattice &La = T->lat[l];
+        if (La.fermion != FERM_STAGGERED) continue;
+        const int lt = tile - La.tile0;
+        const int i = lt * kEngTile + threadIdx.x;
+        const bool valid = i < La.g.Vh;
+        if (threadIdx.x < 32) {
+            const int q = threadIdx.x;
+            int j = 0;
+            bool on = false;
+            if (q < La.nprob) {
+                j = La.prob[q];
+                on = active<PHASE, FERM_STAGGERED_LOW>(P.S[j]);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (on) s_act[__popc(m & ((1u << q) - 1u))] = j;
+            if (q == 0) s_na = __popc(m);
+        }
+        __syncthreads();
+        const int na = s_na;
+        // every tile of a lattice sees the same active slots: a lattice without any is left
+        // alone (no arrival, its ticket untouched)
+        if (na == 0) {
+            __syncthreads();
+            continue;
+        }
+        const LinksF16x18Smem<kEngTile> US{s_lx, s_lz, OUTPAR};
+        SiteNbrs nb;
+        if constexpr (HOP) {
+            if (valid) {
+                nb = site_neighbours(La.g, i, OUTPAR);
+                US.stage(LinksF16x18{La.l16x, La.l16z, La.stride}, nb, i);
+                cp_async_wait_all();
+            }
+        }
+        for (int a = 0; a < na; a++) {
+            const int j = s_act[a];
+            double red[1] = {0.0};
+            if (valid) stag_low_site<PHASE>(La, T->prob[j], P.S[j], US, nb, i, red);
+            if constexpr (NRED > 0) {
+                const double v = warp_sum(red[0]);
+                if ((threadIdx.x & 31) == 0) s_red[a][threadIdx.x >> 5] = v;
+            }
+        }
+        if constexpr (NRED > 0) {
+            __syncthreads();
+            if (threadIdx.x < na) {
+                double sum = 0;
+#pragma unroll
+                for (int w = 0; w < kEngTile / 32; w++) sum += s_red[threadIdx.x][w];
+                P.partials[((size_t)s_act[threadIdx.x] * 2) * max_tiles + lt] = sum;
+                __threadfence();  // visible before the lattice's ticket is taken
+            }
+        }
+        __syncthreads();  // s_act and the staged links are rewritten by the next tile
+        if constexpr (NRED > 0) arrive_and_finish<PHASE, NRED, FERM_STAGGERED_LOW>(P, La, l, smem, last, La.ntiles);
     }
 }
 
@@ -188,10 +268,7 @@ __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
         // the odd FP64 half of the reliable update: t itself, or t64 beside the FP16 t
         const HalfStag t{low ? pr.t64 : static_cast<double2 *>(pr.t), stride};
         double red[2] = {0.0, 0.0};
-        constexpr bool INNER = PHASE == PH_P1 || PHASE == PH_P2 || PHASE == PH_P3 || PHASE == PH_P4 || PHASE == PH_P5;
-        if (i < g.Vh && INNER && low) {
-            stag_low_site<PHASE>(La, pr, st, i, red);
-        } else if (i < g.Vh) {
+        if (i < g.Vh) {
             if constexpr (PHASE == PH_R1) {
                 // first update: record whether the initial x is nonzero anywhere (read by R2, R3)
                 bool nz = false;
@@ -322,10 +399,15 @@ __global__ void __launch_bounds__(kEngTile, 3) k_stag_eng(EngPtrs P) {
 // one iteration of the staggered slots (the reliable-update phases return at once unless
 // some slot asked for one)
 void enqueue_stag_iteration(const EngPtrs &P, const EngGrid &G, cudaStream_t s) {
+    // FP64 and FP16 slots of a phase are disjoint; each kernel finishes its own
     k_stag_eng<PH_P1><<<G.f64, kEngTile, 0, s>>>(P);
+    k_stag_low<PH_P1><<<G.low, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_P2><<<G.f64, kEngTile, 0, s>>>(P);
+    k_stag_low<PH_P2><<<G.low, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_P3><<<G.f64, kEngTile, 0, s>>>(P);
+    k_stag_low<PH_P3><<<G.low, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_P4><<<G.f64, kEngTile, 0, s>>>(P);
+    k_stag_low<PH_P4><<<G.low, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_R1><<<G.f64, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_R2><<<G.f64, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_R3><<<G.f64, kEngTile, 0, s>>>(P);
@@ -334,4 +416,5 @@ void enqueue_stag_iteration(const EngPtrs &P, const EngGrid &G, cudaStream_t s) 
     k_stag_eng<PH_R5><<<G.f64, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_R5L><<<G.f64, kEngTile, 0, s>>>(P);
     k_stag_eng<PH_P5><<<G.f64, kEngTile, 0, s>>>(P);
+    k_stag_low<PH_P5><<<G.low, kEngTile, 0, s>>>(P);
 }
