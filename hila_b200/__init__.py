@@ -75,7 +75,8 @@ class _CgResult(ctypes.Structure):
 
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("delta", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_size_t),
-                ("chunk_iters", ctypes.c_int), ("host_pool_bytes", ctypes.c_size_t)]
+                ("chunk_iters", ctypes.c_int), ("host_pool_bytes", ctypes.c_size_t),
+                ("staggered_precision", ctypes.c_int)]
 
 
 class _RequestResult(ctypes.Structure):
@@ -865,9 +866,9 @@ class Server:
     bitwise the same alone and in any mix."""
 
     def __init__(self, ctx: Context, precision: str = "f16", delta: float = 0.0, hbm_budget_bytes: int = 0,
-                 chunk_iters: int = 8, host_pool_bytes: int = 0):
+                 chunk_iters: int = 8, host_pool_bytes: int = 0, staggered_precision: str = "f64"):
         cfg = _ServerConfig(PRECISIONS[precision], float(delta), int(hbm_budget_bytes), int(chunk_iters),
-                            int(host_pool_bytes))
+                            int(host_pool_bytes), PRECISIONS[staggered_precision])
         self.ctx = ctx
         self.handle = _vp()
         _check(lib().hw_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(self.handle)))

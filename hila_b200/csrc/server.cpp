@@ -327,9 +327,11 @@ int admit_waiting(hw_server *S) {
         for (int k = 0; k < q->nrhs; k++) {
             int slot;
             if (q->mode == REQ_FIELDS) {
-                // the engine reads b and accumulates x in the caller's fields (x: initial guess)
-                // staggered solves are FP64 throughout: a reliable update only confirms convergence
-                const double delta = q->fermion == FERM_STAGGERED ? 0.0 : S->cfg.delta;
+                // the engine reads b and accumulates x in the caller's fields (x: initial guess);
+                // FP64 staggered solves: a reliable update only confirms convergence (delta 0)
+                const double delta = q->fermion != FERM_STAGGERED ? S->cfg.delta
+                                     : S->cfg.staggered_precision == HW_PREC_F16 ? 0.05
+                                                                                 : 0.0;
                 if ((rc = E.admit(l, q->kappa, q->fb[k], q->fx[k], q->tol, q->maxiters, delta, ENG_MODE_SOLVE,
                                   &slot)) != HW_OK)
                     return rc;
@@ -596,6 +598,9 @@ int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server 
     cfg.precision = HW_PREC_F16;
     if (config) cfg = *config;
     HW_CHECK_ARG(cfg.precision == HW_PREC_F16 || cfg.precision == HW_PREC_F32, "server precision must be F16 or F32");
+    HW_CHECK_ARG(cfg.staggered_precision == HW_PREC_F64 ||
+                     (cfg.staggered_precision == HW_PREC_F16 && cfg.precision == HW_PREC_F16),
+                 "staggered precision must be F64, or F16 on an F16 server");
     if (cfg.delta <= 0) cfg.delta = cfg.precision == HW_PREC_F16 ? 0.005 : 1e-5;
     if (cfg.chunk_iters <= 0) cfg.chunk_iters = 8;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);

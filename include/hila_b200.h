@@ -291,6 +291,8 @@ typedef struct hw_server_config {
     size_t hbm_budget_bytes;  /* device memory for solve slots (0: 80% of free memory at creation) */
     int chunk_iters;          /* CG iterations between admission points (<= 0: 8) */
     size_t host_pool_bytes;   /* idle page-locked host buffers the server keeps for reuse (0: 16 GiB) */
+    int staggered_precision;  /* staggered requests: HW_PREC_F64 (0, default) or HW_PREC_F16 (FP16 inner
+                                 iterations, FP64 reliable updates, factor 0.05; needs precision F16) */
 } hw_server_config;
 
 typedef struct hw_request_result {

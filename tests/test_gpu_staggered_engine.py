@@ -147,3 +147,34 @@ def test_staggered_batch_mixed_precision(hw, ctx, oracle):
     ev = oracle.parity_mask(dims) == 0
     x, y = fx.download(), f64.download()
     assert np.linalg.norm(_c(x)[ev] - _c(y)[ev]) / np.linalg.norm(_c(y)[ev]) <= 1e-6
+
+
+def test_staggered_mixed_precision_served(hw, ctx, oracle):
+    """A server with staggered_precision "f16" serves staggered requests with FP16 inner
+    iterations beside Wilson requests; the results reach the oracle's true residual and are
+    bitwise those of the FP16 staggered batch entry point (factor 0.05 in both)."""
+    [(dims, U, lat, G, D, mass, srcs)] = build(hw, ctx, oracle, [((8, 8, 8, 8), 341, 2.4, 2, 18)])
+    Uw = oracle.gen_links((8, 8, 8, 8), 0.3, 342)
+    latw = hw.Lattice(ctx, (8, 8, 8, 8), True)
+    Gw = hw.GaugeField(latw, Uw)
+    bw = [oracle.gen_spinor((8, 8, 8, 8), 343, oracle.EVEN)]
+    srv = hw.Server(ctx, precision="f16", chunk_iters=4, staggered_precision="f16")
+    try:
+        gw, gs = srv.add_gauge(Gw), srv.add_gauge(G)
+        fwb, fwx = [hw.Field(latw, b) for b in bw], [hw.Field(latw) for _ in bw]
+        fsb, fsx = [hw.StaggeredField(lat, b) for b in srcs], [hw.StaggeredField(lat) for _ in srcs]
+        ids = srv.submit_staggered(gs, mass, fsb, fsx, TOL)
+        idw = srv.submit_fields(gw, 0.124, fwb, fwx, TOL)
+        _, rs = srv.wait(ids, 2, lat.volume, copy=False)
+        _, rw = srv.wait(idw, 1, latw.volume, copy=False)
+        assert rw.converged and rs.converged, (rw, rs)
+        assert rs.reliable_updates >= 2, rs
+        for b, f in zip(srcs, fsx):
+            assert residual(oracle, dims, U, mass, b, f.download()) <= TOL
+        alone = [hw.StaggeredField(lat) for _ in srcs]
+        res = hw.staggered_batch_solve(ctx, [(D, fb, fa, TOL) for fb, fa in zip(fsb, alone)], precision="f16")
+        assert all(r.converged for r in res)
+        for a, f in zip(alone, fsx):
+            assert np.array_equal(a.download(), f.download())
+    finally:
+        srv.close()
