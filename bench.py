@@ -33,6 +33,7 @@ host cores, on a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import json
 import os
 import statistics
@@ -676,7 +677,8 @@ def serve_measure(ctx, w, args, rank: int = 0) -> dict:
     torch.cuda.synchronize()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
-    ids, t_sub = [None] * len(reqs), [0.0] * len(reqs)
+    ids, t_sub, t_call = [None] * len(reqs), [0.0] * len(reqs), [0.0] * len(reqs)
+    submitted = [threading.Event() for _ in reqs]
     t0 = time.perf_counter()
 
     def submitter():
@@ -686,27 +688,24 @@ def serve_measure(ctx, w, args, rank: int = 0) -> dict:
                 time.sleep(d)
             t_sub[n] = time.perf_counter()
             ids[n] = srv.submit_eo(gids[g], kappa, [pools[g][k] for k in src], sols_for(g, len(src)), w["tol"])
+            t_call[n] = time.perf_counter() - t_sub[n]
+            submitted[n].set()
+
+    # collect the results with a pool of waiting threads, each blocked in hw_server_wait (the
+    # interpreter lock is released there), so the submitting thread keeps to its schedule and
+    # a slow request holds one waiter, not the others
+    results, t_done = [None] * len(reqs), [0.0] * len(reqs)
+
+    def waiter(n):
+        submitted[n].wait()
+        res = srv.wait(ids[n], len(reqs[n][3]), lats[reqs[n][1]].volume, copy=False)[1]
+        t_done[n] = t_sub[n] + res.latency_seconds
+        results[n] = res
 
     th = threading.Thread(target=submitter)
     th.start()
-    # collect results in completion order, so the server's page-locked solution buffers go
-    # back to its pool as soon as a request is done (a slow request does not hold the others')
-    results, t_done = [None] * len(reqs), [0.0] * len(reqs)
-    pending = set(range(len(reqs)))
-    while pending:
-        got = False
-        for n in sorted(pending):
-            if ids[n] is None:
-                break
-            r = srv.poll(ids[n], len(reqs[n][3]), lats[reqs[n][1]].volume)
-            if r is not None:
-                res = r[1]
-                t_done[n] = t_sub[n] + res.latency_seconds
-                results[n] = res
-                pending.discard(n)
-                got = True
-        if not got:
-            time.sleep(5e-4)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=32) as ex:
+        list(ex.map(waiter, range(len(reqs))))
     th.join()
     clk = clocks.stop()
     st = srv.stats()
@@ -768,11 +767,16 @@ def serve_measure(ctx, w, args, rank: int = 0) -> dict:
         lat.close()
     fifo_capacity = solves / busy
     value = solves / t_wall
+    k_lag = max(range(len(reqs)), key=lambda k: t_sub[k] - (t0 + reqs[k][0]))
     return {
         "value": value, "solves": solves, "requests": len(reqs), "wall_s": t_wall, "clocks": clk,
         "latency_ms_p50": pct(lat_ms, 0.5), "latency_ms_p99": pct(lat_ms, 0.99),
         "queue_ms_p50": pct([1e3 * r.queue_seconds for r in results], 0.5),
         "submit_lag_ms_max": round(1e3 * max(ts - (t0 + r[0]) for ts, r in zip(t_sub, reqs)), 3),
+        "submit_call_ms_max": round(1e3 * max(t_call), 3),
+        "submit_lag_worst": {"request": k_lag, "arrival_s": round(reqs[k_lag][0], 3),
+                             "lattice": "x".join(map(str, w["lattices"][reqs[k_lag][1]])),
+                             "call_ms": round(1e3 * t_call[k_lag], 3)},
         "all_converged": all(r.converged for r in results),
         "max_true_residual": max(r.true_residual for r in results), "spot_check_residual": chk,
         "speedup_vs_fifo_f64_capacity": round(value / fifo_capacity, 3),
@@ -782,6 +786,9 @@ def serve_measure(ctx, w, args, rank: int = 0) -> dict:
         "server_stats": {k: (round(st[k] - st0[k], 3) if k.startswith("seconds") else st[k])
                          for k in ("completed", "solves_completed", "rejected", "cancelled", "seconds_admit",
                                    "seconds_run", "seconds_retire")},
+        # longest single passes of the server thread's sections (warm-up included)
+        "server_max_seconds": {k: round(st[k], 4) for k in ("max_admit_seconds", "max_launch_seconds",
+                                                             "max_retire_seconds")},
         "gpu_launches": int(st["kernel_launches"] - st0["kernel_launches"]),
         "chunks": int(st["chunks"] - st0["chunks"]),
         "bytes_per_request": int(sum(len(r[3]) * lats[r[1]].volume * 96 for r in reqs) / len(reqs)),

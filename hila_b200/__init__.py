@@ -104,7 +104,9 @@ class _ServerStats(ctypes.Structure):
                 ("latency_p50_seconds", ctypes.c_double), ("latency_p99_seconds", ctypes.c_double),
                 ("solves_completed", ctypes.c_uint64), ("chunks", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("seconds_admit", ctypes.c_double),
-                ("seconds_run", ctypes.c_double), ("seconds_retire", ctypes.c_double)]
+                ("seconds_run", ctypes.c_double), ("seconds_retire", ctypes.c_double),
+                ("max_admit_seconds", ctypes.c_double), ("max_launch_seconds", ctypes.c_double),
+                ("max_retire_seconds", ctypes.c_double)]
 
 
 class _SolveRequest(ctypes.Structure):

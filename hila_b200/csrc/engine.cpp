@@ -215,12 +215,37 @@ size_t Engine::slot_bytes_for_stride(int stride) const {
 
 size_t Engine::slot_bytes(int lat) const { return slot_bytes_for_stride(tables_.lat[lat].stride); }
 
+size_t Engine::buffer_bytes(const SlotBuffers &B) {
+    size_t n = 0;
+    for (const DevBuf *d : {&B.p, &B.r, &B.Dp, &B.t, &B.pn, &B.rn, &B.Dpn, &B.tn, &B.y, &B.s, &B.t64, &B.x_own,
+                            &B.b_own, &B.xfer})
+        n += d->bytes;
+    return n;
+}
+
+void Engine::park_buffers(std::unique_ptr<SlotBuffers> B) {
+    const size_t n = buffer_bytes(*B);
+    if (idle_bytes_ + n > kIdleCapBytes) return;  // freed here (the DevBufs release themselves)
+    idle_bytes_ += n;
+    idle_bufs_.emplace(B->stride, std::move(B));
+}
+
 int Engine::ensure_slot_buffers(int slot, int stride) {
-    SlotBuffers &B = bufs_[slot];
-    if (B.stride >= stride && B.p.ptr) return HW_OK;
+    std::unique_ptr<SlotBuffers> &cur = bufs_[slot];
+    if (cur && cur->stride >= stride && cur->p.ptr) return HW_OK;
+    if (cur && cur->p.ptr) park_buffers(std::move(cur));
+    // the smallest idle set that is large enough
+    auto it = idle_bufs_.lower_bound(stride);
+    if (it != idle_bufs_.end()) {
+        idle_bytes_ -= buffer_bytes(*it->second);
+        cur = std::move(it->second);
+        idle_bufs_.erase(it);
+        return HW_OK;
+    }
+    cur.reset(new SlotBuffers());
+    SlotBuffers &B = *cur;
     const size_t st = stride;
     int rc;
-    for (DevBuf *d : {&B.x_own, &B.b_own, &B.xfer}) d->release();
     if (low_ == LOW_F16) {
         for (DevBuf *d : {&B.p, &B.r, &B.Dp, &B.t})
             if ((rc = d->alloc(3 * st * sizeof(uint4))) != HW_OK) return rc;
@@ -239,7 +264,7 @@ int Engine::ensure_slot_buffers(int slot, int stride) {
 }
 
 int Engine::ensure_own(int slot) {
-    SlotBuffers &B = bufs_[slot];
+    SlotBuffers &B = *bufs_[slot];
     const size_t bytes = 12 * (size_t)B.stride * sizeof(double2);
     int rc;
     if (!B.x_own.ptr || B.x_own.bytes < bytes)
@@ -256,12 +281,15 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
     HW_CHECK_ARG(lat >= 0 && lat < tables_.nlat, "bad lattice index");
     EngLattice &L = tables_.lat[lat];
     HW_CHECK_ARG(L.nprob < kEngMaxRhs, "lattice holds %d solves already", kEngMaxRhs);
-    int slot = -1;
-    for (int j = 0; j < kEngMaxProb; j++)
-        if (!slots_[j].used) {
-            slot = j;
-            break;
-        }
+    // a free slot whose buffers fit the lattice with the least to spare, else the first free one
+    int slot = -1, fit = -1;
+    for (int j = 0; j < kEngMaxProb; j++) {
+        if (slots_[j].used) continue;
+        if (slot < 0) slot = j;
+        const SlotBuffers *B = bufs_[j].get();
+        if (B && B->p.ptr && B->stride >= L.stride && (fit < 0 || B->stride < bufs_[fit]->stride)) fit = j;
+    }
+    if (fit >= 0) slot = fit;
     HW_CHECK_ARG(slot >= 0, "no free solve slot (%d in use)", kEngMaxProb);
     int rc;
     // a staggered solve with a reliable-update factor runs its inner iterations in FP16
@@ -274,7 +302,7 @@ int Engine::admit(int lat, double kappa, double2 *b, double2 *x, double tol, int
         L.l16z = gauges_[lat]->f16z.as<unsigned>();
     }
     if ((rc = ensure_slot_buffers(slot, L.stride)) != HW_OK) return rc;
-    SlotBuffers &B = bufs_[slot];
+    SlotBuffers &B = *bufs_[slot];
     if (!b || !x) {
         if ((rc = ensure_own(slot)) != HW_OK) return rc;
         if (!b) b = B.b_own.as<double2>();

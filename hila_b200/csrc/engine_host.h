@@ -2,6 +2,7 @@
 #pragma once
 
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "engine.h"
@@ -48,9 +49,9 @@ class Engine {
     // diag = 1 + m_h solves with the Hasenbusch operator M + m_h (1: M itself).
     int admit(int lat, double kappa, double2 *b, double2 *x, double tol, int maxiter, double delta, int mode,
               int *slot, double diag = 1.0);
-    double2 *own_b(int slot) { return bufs_[slot].b_own.as<double2>(); }
-    double2 *own_x(int slot) { return bufs_[slot].x_own.as<double2>(); }
-    double2 *own_xfer(int slot) { return bufs_[slot].xfer.as<double2>(); }
+    double2 *own_b(int slot) { return bufs_[slot]->b_own.as<double2>(); }
+    double2 *own_x(int slot) { return bufs_[slot]->x_own.as<double2>(); }
+    double2 *own_xfer(int slot) { return bufs_[slot]->xfer.as<double2>(); }
     int ensure_own(int slot);
     // stream-ordered: run up to `iters` iterations of every running slot
     // (stops early when none runs)
@@ -96,7 +97,16 @@ class Engine {
     EngTables tables_{};
     std::vector<const hw_gauge *> gauges_;
     SlotInfo slots_[kEngMaxProb];
-    SlotBuffers bufs_[kEngMaxProb];
+    std::unique_ptr<SlotBuffers> bufs_[kEngMaxProb];
+    // Slot buffers set aside by a slot that took a lattice of another size, by stride.  A
+    // slot whose buffers are too small swaps them for idle ones before anything is
+    // allocated: cudaMalloc and cudaFree synchronise the device, and a server admitting
+    // requests of many lattice sizes stalled on them.  Idle buffers beyond the cap are freed.
+    std::multimap<int, std::unique_ptr<SlotBuffers>> idle_bufs_;
+    size_t idle_bytes_ = 0;
+    static constexpr size_t kIdleCapBytes = size_t(16) << 30;
+    static size_t buffer_bytes(const SlotBuffers &B);
+    void park_buffers(std::unique_ptr<SlotBuffers> B);
     EngState host_states_[kEngMaxProb];
     EngState *pinned_states_ = nullptr;
     int *pinned_ctl_ = nullptr;

@@ -560,10 +560,13 @@ void server_loop(hw_server *S) {
         auto since = [](Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); };
         Clock::time_point t0 = Clock::now();
         int rc = admit_waiting(S);
-        S->stats.seconds_admit += since(t0);
+        double dt = since(t0);
+        S->stats.seconds_admit += dt;
+        S->stats.max_admit_seconds = std::max(S->stats.max_admit_seconds, dt);
         if (rc == HW_OK && !S->running.empty()) {
             t0 = Clock::now();
             rc = S->eng->launch_chunk(S->cfg.chunk_iters);
+            S->stats.max_launch_seconds = std::max(S->stats.max_launch_seconds, since(t0));
             if (rc == HW_OK) {
                 // clients can submit and wait while the chunk runs on the device
                 lk.unlock();
@@ -579,7 +582,9 @@ void server_loop(hw_server *S) {
         if (rc == HW_OK) rc = retire_finished(S);
         // with nothing left on the engine, wait for the oldest copies instead of spinning
         if (rc == HW_OK) rc = finish_rounds(S, S->running.empty() && S->queue.empty());
-        S->stats.seconds_retire += since(t0);
+        dt = since(t0);
+        S->stats.seconds_retire += dt;
+        S->stats.max_retire_seconds = std::max(S->stats.max_retire_seconds, dt);
         if (rc != HW_OK) fail_all(S, rc);
     }
 }

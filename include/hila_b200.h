@@ -318,6 +318,9 @@ typedef struct hw_server_stats {
     double seconds_admit;                              /* server-thread wall time admitting requests */
     double seconds_run;                                /* ... launching chunks and reading slot states */
     double seconds_retire;                             /* ... copying solutions out and retiring */
+    /* the longest single pass of each server-thread section; submissions wait for the
+     * server lock while one runs (admission, chunk launch, retirement) */
+    double max_admit_seconds, max_launch_seconds, max_retire_seconds;
 } hw_server_stats;
 
 int hw_server_create(hw_context *ctx, const hw_server_config *config, hw_server **server);
