@@ -230,6 +230,13 @@ void Engine::park_buffers(std::unique_ptr<SlotBuffers> B) {
     idle_bufs_.emplace(B->stride, std::move(B));
 }
 
+void Engine::free_idle() {
+    if (idle_bufs_.empty()) return;
+    cudaStreamSynchronize(ctx_->stream);
+    idle_bufs_.clear();
+    idle_bytes_ = 0;
+}
+
 int Engine::ensure_slot_buffers(int slot, int stride) {
     std::unique_ptr<SlotBuffers> &cur = bufs_[slot];
     if (cur && cur->stride >= stride && cur->p.ptr) return HW_OK;
@@ -242,6 +249,17 @@ int Engine::ensure_slot_buffers(int slot, int stride) {
         idle_bufs_.erase(it);
         return HW_OK;
     }
+    if (stride < min_stride_) stride = min_stride_;
+    int rc = alloc_slot_buffers(cur, stride);
+    if (rc == HW_ERR_OOM && !idle_bufs_.empty()) {  // give the idle sets back and try once more
+        clear_error();
+        free_idle();
+        rc = alloc_slot_buffers(cur, stride);
+    }
+    return rc;
+}
+
+int Engine::alloc_slot_buffers(std::unique_ptr<SlotBuffers> &cur, int stride) {
     cur.reset(new SlotBuffers());
     SlotBuffers &B = *cur;
     const size_t st = stride;

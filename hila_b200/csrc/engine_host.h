@@ -72,6 +72,9 @@ class Engine {
     // device bytes of one solve slot (including slot-owned b and x) for a lattice stride
     size_t slot_bytes_for_stride(int stride) const;
     int slot_lattice(int slot) const { return slots_[slot].lat; }
+    // Size every slot's buffers for at least this stride when they are first made, so a slot
+    // can later take any lattice up to it without allocating (0: each lattice's own stride)
+    void set_min_stride(int stride) { min_stride_ = stride; }
     const EngLattice &lattice(int l) const { return tables_.lat[l]; }
     int nlat() const { return tables_.nlat; }
     const hw_gauge *gauge(int l) const { return gauges_[l]; }
@@ -104,6 +107,9 @@ class Engine {
     // requests of many lattice sizes stalled on them.  Idle buffers beyond the cap are freed.
     std::multimap<int, std::unique_ptr<SlotBuffers>> idle_bufs_;
     size_t idle_bytes_ = 0;
+    int min_stride_ = 0;
+    void free_idle();
+    int alloc_slot_buffers(std::unique_ptr<SlotBuffers> &cur, int stride);
     static constexpr size_t kIdleCapBytes = size_t(16) << 30;
     static size_t buffer_bytes(const SlotBuffers &B);
     void park_buffers(std::unique_ptr<SlotBuffers> B);

@@ -674,6 +674,12 @@ int hw_server_add_gauge(hw_server *S, const hw_gauge *gauge, int *gauge_id) {
     tune_hop(gauge->lat, gauge);
     S->gauges.push_back(G);
     *gauge_id = (int)S->gauges.size() - 1;
+    // slots sized for the largest lattice when every slot fits in half the budget: a slot
+    // then takes any lattice without allocating (allocation stalls the device mid-stream)
+    int max_stride = 0;
+    for (const GaugeEntry &e : S->gauges) max_stride = std::max(max_stride, padded_stride(e.Vh));
+    const size_t all_slots = (size_t)kEngMaxProb * S->eng->slot_bytes_for_stride(max_stride);
+    S->eng->set_min_stride(all_slots <= S->cfg.hbm_budget_bytes / 2 ? max_stride : 0);
     return HW_OK;
 }
 
