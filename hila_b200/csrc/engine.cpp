@@ -256,6 +256,7 @@ int Engine::ensure_slot_buffers(int slot, int stride) {
         free_idle();
         rc = alloc_slot_buffers(cur, stride);
     }
+    if (rc != HW_OK) cur.reset();  // no half-made set stays with the slot
     return rc;
 }
 
