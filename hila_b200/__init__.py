@@ -208,6 +208,9 @@ _SIGNATURES = {
 _lib = None
 
 
+API_VERSION = 2  # HW_API_VERSION of include/hila_b200.h whose structs this binding mirrors
+
+
 def load_library() -> ctypes.CDLL:
     """Load libhila_b200.so; raises ImportError if it has not been built."""
     global _lib
@@ -220,6 +223,9 @@ def load_library() -> ctypes.CDLL:
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        if L.hw_api_version() != API_VERSION:
+            raise ImportError(f"{LIB_PATH} has API version {L.hw_api_version()}, this binding expects "
+                              f"{API_VERSION}: rebuild it with `python -m hila_b200.build`")
         _lib = L
     return _lib
 

@@ -33,7 +33,9 @@
 extern "C" {
 #endif
 
-#define HW_API_VERSION 1
+/* 2: hw_stag_solve_request.precision / delta, hw_server_config.staggered_precision,
+ *    hw_server_stats maxima, hw_engine_tuning (struct layouts changed) */
+#define HW_API_VERSION 2
 
 enum hw_status {
     HW_OK = 0,

@@ -43,8 +43,8 @@ def test_python_binding_covers_header(hw, lib):
     assert not missing, f"python binding lacks {sorted(missing)}"
 
 
-def test_api_version(lib):
-    assert lib.hw_api_version() == 1
+def test_api_version(hw, lib):
+    assert lib.hw_api_version() == hw.API_VERSION == 2
 
 
 def test_no_device_fails_loudly(hw, lib):
@@ -106,6 +106,6 @@ def test_header_is_c99_and_links_from_c(hw, lib, tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert run.returncode == 0, run.stderr
     version, rc, first, last = run.stdout.split()
-    assert int(rc) == 0 and int(version) >= 1
+    assert int(rc) == 0 and int(version) == hw.API_VERSION
     U = hw.generate_links((4, 4, 4, 2), 0.3, 7)
     assert float(first) == U.reshape(-1)[0] and float(last) == U.reshape(-1)[-1]
